@@ -1,0 +1,70 @@
+/*
+ * ops_b200_loop.h -- ABI between translator-generated par_loop stubs and the
+ * host runtime.
+ *
+ * Replaces the per-loop host logic of the reference's generated CUDA stub
+ * (ops_translator/resources/templates/cpp/cuda/loop_host.cpp.j2:13-780):
+ * range/start computation, H->D dirty-bit exchange, reduction staging,
+ * base-pointer computation, dirty-bit update and timing.  The stub calls
+ * ob2_loop_begin, launches its own kernel with the views it gets back, and
+ * calls ob2_loop_end.
+ */
+#ifndef OPS_B200_LOOP_H
+#define OPS_B200_LOOP_H
+
+#include "ops_lib_core.h"
+#include "ops_b200_device.h"
+
+#define OB2_MAX_ARGS 48
+
+/* Where one dat argument lives for the loop:
+ *   element of loop point (x,y,z) = base + x*wx + y*wy + z*wz   (elements)
+ *   ACC strides ex/ey/ez/ed: neighbours along x/y/z and between components. */
+typedef struct ob2_view {
+  char *base;
+  long long wx, wy, wz;
+  int ex, ey, ez, ed;
+} ob2_view;
+
+/* reduction target of one ops_arg_reduce */
+typedef struct ob2_red {
+  void *acc;    /* device accumulator of the handle (dim values) */
+  int first;    /* 1: this loop initialises the accumulator */
+  int op;       /* OPS_INC / OPS_MIN / OPS_MAX */
+} ob2_red;
+
+typedef struct ob2_loop {
+  const char *name;
+  int kernel_index;  /* timing-table slot */
+  int dim;
+  int lo[3], hi[3];
+  int n[3];          /* hi - lo (clamped at 0) */
+  long long npoints;
+  void *stream;
+  int nargs;
+  ops_arg *args;
+  ob2_view view[OB2_MAX_ARGS];
+  ob2_red red[OB2_MAX_ARGS];
+  void *partials;           /* device scratch: per-CTA reduction partials */
+  size_t partials_bytes;
+  unsigned int *counter;    /* device: CTAs finished (last-CTA combine) */
+  void *ev_start, *ev_end;  /* timing events (diagnostics level > 1) */
+  double host_t0;
+  int block[3];             /* suggested CTA shape */
+} ob2_loop;
+
+/* Returns 0 when the range is empty (nothing to launch, ob2_loop_end not
+ * needed), 1 otherwise. */
+OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int dim,
+                           const int *range, ops_arg *args, int nargs);
+OPS_API void ob2_loop_end(ob2_loop *L);
+/* Checks the launch just issued; throws OPSException on error. */
+OPS_API void ob2_loop_check_launch(ob2_loop *L);
+
+/* Constant registry: the generated kernels file registers one callback that
+ * copies a named constant into its __constant__ symbol. */
+typedef int (*ob2_const_fn)(const char *name, int dim, int type_size, const char *data,
+                            void *stream);
+OPS_API void ob2_register_const_handler(ob2_const_fn fn);
+
+#endif /* OPS_B200_LOOP_H */

@@ -1,0 +1,1246 @@
+// ob2_runtime.cpp -- the OPS host runtime of the B200 backend.
+//
+// Implements the C entry points of include/ops_lib_core.h (and the
+// generated-stub ABI of include/ops_b200_loop.h) on top of the thin CUDA ABI
+// of include/ops_b200_device.h.  Replaces, for a single GPU:
+//   ops/c/src/core/ops_lib_core.cpp      object declaration, args, reductions,
+//                                        dirty bits, timing/transfer model
+//   ops/c/src/core/ops_device_singlenode_common.cpp   device dats, halo transfer
+//   ops/c/src/core/ops_dummy_singlenode.cpp           raw pointers, fetch/set,
+//                                        low-dim (edge) dat accumulation init
+//   ops/c/src/cuda/ops_cuda_common.cu    device init, memory, random fills
+//
+// Design: every dat lives in HBM (device copy authoritative); the host copy is
+// materialised only when the app asks for host data.  Par_loops, halo
+// transfers and tridiagonal solves are queued on one CUDA stream and never
+// wait for the device; only reduction results, fetches and host raw pointers
+// synchronise.  Errors surface as OPSException with the reference's codes.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <limits>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "ops_b200_device.h"
+#include "ops_b200_loop.h"
+#include "ops_lib_core.h"
+#include "ops_tridiag.h"
+
+namespace {
+
+struct KStat {
+  std::string name;
+  long count = 0;
+  double host_s = 0.0;    // host wall time (enqueue, or device time under diags>1)
+  double dev_ms = 0.0;    // device time from events (diags > 1)
+  double transfer = 0.0;  // bytes, OPS transfer model
+};
+
+struct DatX {
+  int edat_prev_acc = -1;  // last access kind of an edge dat
+};
+
+struct RedX {
+  void *acc_d = nullptr;   // device accumulator
+  int pending_first = 0;   // next loop initialises the accumulator
+  void *host_pinned = nullptr;
+};
+
+struct GroupX {
+  void *tasks_d = nullptr;
+  int ntasks = 0;
+  long long max_pts = 0;
+  std::vector<char *> key;  // dat device pointers the table was built for
+};
+
+struct Runtime {
+  OPS_instance inst;
+  bool initialised = false;
+  std::vector<ops_block> blocks;
+  std::vector<ops_dat> dats;
+  std::vector<DatX> datx;
+  std::vector<ops_stencil> stencils;
+  std::vector<ops_halo> halos;
+  std::vector<ops_halo_group> groups;
+  std::vector<GroupX> groupx;
+  std::vector<ops_reduction> reds;
+  std::vector<RedX> redx;
+  std::vector<KStat> kstats;
+  std::unordered_map<std::string, int> kindex;
+  int block_x = 32, block_y = 4, block_z = 1;
+  int device = 0;
+  // reduction scratch: per-CTA partials + finish counter
+  void *partials = nullptr;
+  size_t partials_cap = 0;
+  unsigned int *counter = nullptr;
+  // staging buffer for fetch / set
+  char *stage_d = nullptr;
+  size_t stage_cap = 0;
+  unsigned long long rng_seed = 0, rng_counter = 0;
+  ob2_const_fn const_fn = nullptr;
+  ob2_loop *loop_events = nullptr;
+};
+
+Runtime *R = nullptr;
+
+Runtime &rt() {
+  if (!R) {
+    R = new Runtime();
+    memset((void *)&R->inst, 0, sizeof(R->inst));
+  }
+  return *R;
+}
+
+void check(int code, const char *what) {
+  if (code != 0) {
+    OPSException ex(OPS_RUNTIME_ERROR);
+    ex << "Error: CUDA error in " << what << ": " << ob2_error_string(code);
+    throw ex;
+  }
+}
+
+void require_init() {
+  if (!rt().initialised) {
+    throw OPSException(OPS_RUNTIME_CONFIGURATION_ERROR,
+                       "Error: ops_init must be called before other OPS routines");
+  }
+}
+
+char *copy_str(const char *s) {
+  if (!s) return nullptr;
+  size_t n = strlen(s);
+  char *r = (char *)malloc(n + 1);
+  memcpy(r, s, n + 1);
+  return r;
+}
+
+double wall() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+size_t dat_points(ops_dat d) {
+  size_t n = 1;
+  for (int i = 0; i < OPS_MAX_DIM; i++) n *= (size_t)d->size[i];
+  return n;
+}
+
+void ensure_host(ops_dat d) {
+  if (!d->data) {
+    d->data = (char *)calloc(d->mem ? d->mem : 1, 1);
+    d->user_managed = 0;
+  }
+}
+
+/* device -> host when the device copy is newer (ops_lib_core.cpp:2366-2379) */
+void get_data(ops_dat d) {
+  ensure_host(d);
+  if (d->dirty_hd == 2) {
+    check(ob2_dev_d2h(d->data, d->data_d, d->mem), "ops_get_data");
+    d->dirty_hd = 0;
+  }
+}
+
+/* host -> device when the host copy is newer (ops_lib_core.cpp:2381-2392) */
+void put_data(ops_dat d) {
+  if (d->dirty_hd == 1) {
+    check(ob2_dev_h2d(d->data_d, d->data, d->mem), "ops_put_data");
+    d->dirty_hd = 0;
+  }
+}
+
+int type_code(const char *t) {
+  if (!strcmp(t, "double") || !strcmp(t, "real(8)") || !strcmp(t, "double precision")) return 1;
+  if (!strcmp(t, "float") || !strcmp(t, "real") || !strcmp(t, "real(4)")) return 2;
+  if (!strcmp(t, "int") || !strcmp(t, "integer") || !strcmp(t, "int(4)")) return 3;
+  if (!strcmp(t, "long long") || !strcmp(t, "ll")) return 4;
+  if (!strcmp(t, "unsigned int") || !strcmp(t, "uint")) return 5;
+  if (!strcmp(t, "char")) return 6;
+  if (!strcmp(t, "short")) return 7;
+  if (!strcmp(t, "long")) return 8;
+  return 0;
+}
+
+/* identity of a reduction / low-dim accumulation (ops_lib_core.cpp:840-965) */
+void identity_bytes(int tc, int acc, void *out, bool lowdim) {
+  switch (tc) {
+    case 1: {
+      double v = acc == OPS_MIN ? DBL_MAX : (acc == OPS_MAX ? -DBL_MAX : 0.0);
+      if (lowdim && acc == OPS_MAX) v = std::numeric_limits<double>::lowest();
+      memcpy(out, &v, 8);
+      break;
+    }
+    case 2: {
+      float v = acc == OPS_MIN ? FLT_MAX : (acc == OPS_MAX ? -FLT_MAX : 0.0f);
+      memcpy(out, &v, 4);
+      break;
+    }
+    case 3: {
+      int v = acc == OPS_MIN ? INT_MAX : (acc == OPS_MAX ? INT_MIN : 0);
+      memcpy(out, &v, 4);
+      break;
+    }
+    case 4: {
+      long long v = acc == OPS_MIN ? LLONG_MAX : (acc == OPS_MAX ? LLONG_MIN : 0);
+      memcpy(out, &v, 8);
+      break;
+    }
+    case 5: {
+      unsigned v = acc == OPS_MIN ? UINT_MAX : 0u;
+      memcpy(out, &v, 4);
+      break;
+    }
+    case 6: {
+      char v = acc == OPS_MIN ? CHAR_MAX : (acc == OPS_MAX ? CHAR_MIN : 0);
+      memcpy(out, &v, 1);
+      break;
+    }
+    case 7: {
+      short v = acc == OPS_MIN ? SHRT_MAX : (acc == OPS_MAX ? SHRT_MIN : 0);
+      memcpy(out, &v, 2);
+      break;
+    }
+    case 8: {
+      long v = acc == OPS_MIN ? LONG_MAX : (acc == OPS_MAX ? LONG_MIN : 0);
+      memcpy(out, &v, 8);
+      break;
+    }
+    default:
+      throw OPSException(OPS_NOT_IMPLEMENTED, "Error, reduction type not recognised");
+  }
+}
+
+int kernel_slot(const char *name) {
+  Runtime &r = rt();
+  auto it = r.kindex.find(name);
+  if (it != r.kindex.end()) return it->second;
+  int k = (int)r.kstats.size();
+  r.kstats.push_back(KStat());
+  r.kstats.back().name = name;
+  r.kindex[name] = k;
+  return k;
+}
+
+}  // namespace
+
+OPS_instance *OPS_instance::getOPSInstance() { return &rt().inst; }
+
+/* ------------------------------------------------------------------------
+ * init / exit  (ops_lib_core.cpp:100-275; ops_cuda_common.cu:68-182)
+ * ---------------------------------------------------------------------- */
+OPS_API void ops_init(const int argc, const char *const argv[], const int diags) {
+  Runtime &r = rt();
+  r.inst.OPS_diags = diags;
+  r.inst.OPS_hybrid_gpu = 1;
+  for (int i = 0; i < argc; i++) {
+    if (!argv || !argv[i]) continue;
+    const char *a = argv[i];
+    const char *p;
+    if ((p = strstr(a, "-OPS_DIAGS="))) r.inst.OPS_diags = atoi(p + 11);
+    if ((p = strstr(a, "OPS_BLOCK_SIZE_X="))) r.block_x = atoi(p + 17);
+    if ((p = strstr(a, "OPS_BLOCK_SIZE_Y="))) r.block_y = atoi(p + 17);
+    if ((p = strstr(a, "OPS_BLOCK_SIZE_Z="))) r.block_z = atoi(p + 17);
+    if ((p = strstr(a, "OPS_DEVICE="))) r.device = atoi(p + 11);
+  }
+  const char *e;
+  if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
+  if (r.block_x < 1) r.block_x = 32;
+  if (r.block_y < 1) r.block_y = 1;
+  if (r.block_z < 1) r.block_z = 1;
+  if (r.initialised) return;
+  check(ob2_dev_init(r.device), "ops_init (no usable CUDA device)");
+  check(ob2_dev_malloc((void **)&r.counter, 4096), "ops_init");
+  check(ob2_dev_memset(r.counter, 0, 4096), "ops_init");
+  r.initialised = true;
+}
+
+OPS_API void ops_dump_dats(const char *path);
+
+OPS_API void ops_exit(void) {
+  if (!R || !R->initialised) return;
+  const char *dump = getenv("OPS_DUMP_FILE");
+  if (dump && *dump) ops_dump_dats(dump);
+  ob2_dev_sync();
+}
+
+OPS_API void ops_set_soa(const int soa) { rt().inst.OPS_soa = soa; }
+
+OPS_API ops_block ops_decl_block(int dims, const char *name) {
+  if (dims < 1 || dims > 3)
+    throw OPSException(OPS_INVALID_ARGUMENT,
+                       "Error: ops_decl_block -- this backend supports 1D, 2D and 3D blocks");
+  ops_block b = (ops_block)calloc(1, sizeof(ops_block_core));
+  b->dims = dims;
+  b->name = copy_str(name);
+  b->instance = &rt().inst;
+  b->index = (int)rt().blocks.size();
+  rt().blocks.push_back(b);
+  return b;
+}
+
+/* ------------------------------------------------------------------------
+ * dats (ops_lib_core.cpp:445-601; ops_device_singlenode_common.cpp:45-106)
+ * ---------------------------------------------------------------------- */
+OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base, int *d_m,
+                                  int *d_p, int *stride, char *data, int type_size,
+                                  char const *type, char const *name) {
+  require_init();
+  if (dim <= 0) {
+    OPSException ex(OPS_INVALID_ARGUMENT);
+    ex << "Error: ops_decl_dat -- negative/zero number of items per grid point in dataset: "
+       << name;
+    throw ex;
+  }
+  ops_dat d = (ops_dat)calloc(1, sizeof(ops_dat_core));
+  d->block = block;
+  d->dim = dim;
+  d->type_size = type_size;
+  d->elem_size = dim * type_size;
+  for (int n = 0; n < OPS_MAX_DIM; n++) {
+    d->size[n] = 1;
+    d->stride[n] = 1;
+  }
+  for (int n = 0; n < block->dims; n++) {
+    if (d_m[n] > 0) {
+      OPSException ex(OPS_INVALID_ARGUMENT);
+      ex << "Error: ops_decl_dat -- Non negative d_m during declaration of: " << name;
+      throw ex;
+    }
+    if (d_p[n] < 0) {
+      OPSException ex(OPS_INVALID_ARGUMENT);
+      ex << "Error: ops_decl_dat -- Non positive d_p during declaration of: " << name;
+      throw ex;
+    }
+    if (size[n] != 1) {
+      d->size[n] = size[n] - d_m[n] + d_p[n];
+      d->base[n] = base[n];
+    } else {
+      d->size[n] = 1;
+      d->e_dat = 1;
+      d->base[n] = 0;
+    }
+    d->d_m[n] = d_m[n];
+    d->d_p[n] = d_p[n];
+    d->stride[n] = stride ? stride[n] : 1;
+  }
+  d->type = copy_str(type);
+  d->name = copy_str(name);
+  d->mem = (size_t)d->elem_size * dat_points(d);
+  check(ob2_dev_malloc((void **)&d->data_d, d->mem), "ops_decl_dat (device allocation)");
+  if (data) {
+    d->data = data;
+    d->user_managed = 1;
+    check(ob2_dev_h2d(d->data_d, data, d->mem), "ops_decl_dat (upload)");
+  } else {
+    d->data = nullptr;
+    d->user_managed = 0;
+    check(ob2_dev_memset(d->data_d, 0, d->mem), "ops_decl_dat (zero)");
+  }
+  d->dirty_hd = data ? 0 : 2;
+  long long off = 0, cum = 1;
+  for (int i = 0; i < block->dims; i++) {
+    off += (long long)(rt().inst.OPS_soa ? d->type_size : d->elem_size) * cum *
+           (-d->base[i] - d->d_m[i]);
+    cum *= d->size[i];
+  }
+  d->base_offset = (size_t)off;
+  d->index = (int)rt().dats.size();
+  rt().dats.push_back(d);
+  rt().datx.push_back(DatX());
+  return d;
+}
+
+OPS_API void ops_free_dat(ops_dat d) {
+  if (!d) return;
+  ob2_dev_sync();
+  for (auto &p : rt().dats)
+    if (p == d) p = nullptr;
+  ob2_dev_free(d->data_d);
+  if (!d->user_managed) free(d->data);
+  free(d);
+}
+
+OPS_API void ops_dat_deep_copy(ops_dat target, ops_dat src) {
+  require_init();
+  if (target->data_d && target->mem != src->mem) {
+    ob2_dev_sync();
+    ob2_dev_free(target->data_d);
+    target->data_d = nullptr;
+  }
+  if (!target->data_d) check(ob2_dev_malloc((void **)&target->data_d, src->mem), "deep copy");
+  if (target->data && !target->user_managed) free(target->data);
+  char *dd = target->data_d;
+  int idx = target->index;
+  ops_block blk = target->block ? target->block : src->block;
+  memcpy(target, src, sizeof(ops_dat_core));
+  target->data_d = dd;
+  target->data = nullptr;
+  target->user_managed = 0;
+  target->index = idx;
+  target->block = blk;
+  target->name = copy_str(src->name);
+  target->type = copy_str(src->type);
+  put_data(src);
+  check(ob2_dev_d2d(target->data_d, src->data_d, src->mem), "deep copy");
+  target->dirty_hd = 2;
+  target->locked_hd = 0;
+}
+
+OPS_API ops_dat ops_dat_copy(ops_dat src) {
+  ops_dat d = (ops_dat)calloc(1, sizeof(ops_dat_core));
+  d->block = src->block;
+  d->index = (int)rt().dats.size();
+  rt().dats.push_back(d);
+  rt().datx.push_back(DatX());
+  ops_dat_deep_copy(d, src);
+  return d;
+}
+
+/* ------------------------------------------------------------------------
+ * args (ops_lib_core.cpp:856-1105)
+ * ---------------------------------------------------------------------- */
+OPS_API ops_arg ops_arg_dat(ops_dat dat, int dim, ops_stencil stencil, char const *,
+                            ops_access acc) {
+  ops_arg a;
+  memset(&a, 0, sizeof(a));
+  if (acc == OPS_WRITE && stencil && stencil->points != 1)
+    throw OPSException(OPS_INVALID_ARGUMENT,
+                       "Error: OPS does not support OPS_WRITE arguments with a non (0,0,0) "
+                       "stencil due to potential race conditions");
+  a.argtype = OPS_ARG_DAT;
+  a.dat = dat;
+  a.stencil = stencil;
+  a.dim = dim;
+  a.acc = acc;
+  a.opt = 1;
+  if (dat) {
+    a.data = dat->data;
+    a.data_d = dat->data_d;
+    a.elem_size = dat->elem_size;
+  }
+  return a;
+}
+
+OPS_API ops_arg ops_arg_dat_opt(ops_dat dat, int dim, ops_stencil stencil, char const *type,
+                                ops_access acc, int flag) {
+  ops_arg a = ops_arg_dat(dat, dim, stencil, type, acc);
+  a.opt = flag;
+  return a;
+}
+
+OPS_API ops_arg ops_arg_idx(void) {
+  ops_arg a;
+  memset(&a, 0, sizeof(a));
+  a.argtype = OPS_ARG_IDX;
+  return a;
+}
+
+OPS_API ops_arg ops_arg_gbl_char(char *data, int dim, int size, ops_access acc) {
+  ops_arg a;
+  memset(&a, 0, sizeof(a));
+  a.argtype = OPS_ARG_GBL;
+  a.data = data;
+  a.dim = dim;
+  a.elem_size = size;
+  a.acc = acc;
+  return a;
+}
+
+OPS_API ops_arg ops_arg_reduce(ops_reduction h, int dim, const char *type, ops_access acc) {
+  ops_arg a;
+  memset(&a, 0, sizeof(a));
+  a.argtype = OPS_ARG_GBL;
+  a.dim = dim;
+  a.data = (char *)h;
+  a.acc = acc;
+  if (!h->initialized) {
+    h->initialized = 1;
+    h->acc = acc;
+    int tc = type_code(type);
+    int ts = tc == 1 || tc == 4 || tc == 8 ? 8 : (tc == 6 ? 1 : (tc == 7 ? 2 : 4));
+    for (int off = 0; off + ts <= h->size; off += ts) identity_bytes(tc, acc, h->data + off, false);
+    rt().redx[h->index].pending_first = 1;
+  } else if (h->acc != acc) {
+    OPSException ex(OPS_INVALID_ARGUMENT);
+    ex << "Error: ops_reduction handle " << h->name
+       << " was already used with a different access type";
+    throw ex;
+  }
+  return a;
+}
+
+OPS_API ops_reduction ops_decl_reduction_handle(int size, const char *type, const char *name) {
+  require_init();
+  ops_reduction r = (ops_reduction)calloc(1, sizeof(ops_reduction_core));
+  r->size = size;
+  r->data = (char *)calloc(size, 1);
+  r->type = copy_str(type);
+  r->name = copy_str(name);
+  r->instance = &rt().inst;
+  r->index = (int)rt().reds.size();
+  rt().reds.push_back(r);
+  RedX x;
+  check(ob2_dev_malloc(&x.acc_d, size > 0 ? size : 8), "ops_decl_reduction_handle");
+  check(ob2_host_alloc_pinned(&x.host_pinned, size > 0 ? size : 8), "ops_decl_reduction_handle");
+  rt().redx.push_back(x);
+  return r;
+}
+
+/* ops_lib_core.cpp:1143-1149: forces execution, returns, resets the handle */
+OPS_API void ops_reduction_result_char(ops_reduction h, int, char *ptr) {
+  RedX &x = rt().redx[h->index];
+  if (!x.pending_first) {
+    check(ob2_dev_d2h_async(x.host_pinned, x.acc_d, h->size), "ops_reduction_result");
+    check(ob2_dev_sync(), "ops_reduction_result");
+    memcpy(h->data, x.host_pinned, h->size);
+  }
+  memcpy(ptr, h->data, h->size);
+  x.pending_first = 0;
+  h->initialized = 0;
+}
+
+/* ------------------------------------------------------------------------
+ * stencils (ops_lib_core.cpp:640-836)
+ * ---------------------------------------------------------------------- */
+static ops_stencil make_stencil(int dims, int points, int *sten, int *stride, const char *name,
+                                int type) {
+  ops_stencil s = (ops_stencil)calloc(1, sizeof(ops_stencil_core));
+  s->dims = dims;
+  s->points = points;
+  s->name = copy_str(name);
+  s->stencil = (int *)malloc(sizeof(int) * (size_t)(dims * points > 0 ? dims * points : 1));
+  if (dims * points > 0) memcpy(s->stencil, sten, sizeof(int) * dims * points);
+  s->stride = (int *)malloc(sizeof(int) * OPS_MAX_DIM);
+  s->mgrid_stride = (int *)malloc(sizeof(int) * OPS_MAX_DIM);
+  for (int i = 0; i < OPS_MAX_DIM; i++) {
+    s->stride[i] = (stride && i < dims) ? stride[i] : 1;
+    s->mgrid_stride[i] = 1;
+  }
+  s->type = type;
+  s->index = (int)rt().stencils.size();
+  rt().stencils.push_back(s);
+  return s;
+}
+OPS_API ops_stencil ops_decl_stencil(int dims, int points, int *sten, char const *name) {
+  return make_stencil(dims, points, sten, nullptr, name, 0);
+}
+OPS_API ops_stencil ops_decl_strided_stencil(int dims, int points, int *sten, int *stride,
+                                             char const *name) {
+  return make_stencil(dims, points, sten, stride, name, 0);
+}
+OPS_API ops_stencil ops_decl_restrict_stencil(int, int, int *, int *, char const *) {
+  throw OPSException(OPS_NOT_IMPLEMENTED,
+                     "Error: multigrid restrict stencils are not supported by this backend");
+}
+OPS_API ops_stencil ops_decl_prolong_stencil(int, int, int *, int *, char const *) {
+  throw OPSException(OPS_NOT_IMPLEMENTED,
+                     "Error: multigrid prolong stencils are not supported by this backend");
+}
+
+/* ------------------------------------------------------------------------
+ * halos (ops_lib_core.cpp:967-1045; ops_device_singlenode_common.cpp:262-346)
+ * ---------------------------------------------------------------------- */
+OPS_API ops_halo ops_decl_halo(ops_dat from, ops_dat to, int *iter_size, int *from_base,
+                               int *to_base, int *from_dir, int *to_dir) {
+  ops_halo h = (ops_halo)calloc(1, sizeof(ops_halo_core));
+  h->from = from;
+  h->to = to;
+  for (int i = 0; i < OPS_MAX_DIM; i++) {
+    bool used = i < from->block->dims;
+    h->iter_size[i] = used ? iter_size[i] : 1;
+    h->from_base[i] = used ? from_base[i] : 0;
+    h->to_base[i] = used ? to_base[i] : 0;
+    h->from_dir[i] = used ? from_dir[i] : i + 1;
+    h->to_dir[i] = used ? to_dir[i] : i + 1;
+  }
+  h->index = (int)rt().halos.size();
+  rt().halos.push_back(h);
+  return h;
+}
+
+OPS_API ops_halo_group ops_decl_halo_group(int nhalos, ops_halo *halos) {
+  ops_halo_group g = (ops_halo_group)calloc(1, sizeof(ops_halo_group_core));
+  g->nhalos = nhalos;
+  g->halos = (ops_halo *)malloc(sizeof(ops_halo) * (nhalos > 0 ? nhalos : 1));
+  for (int i = 0; i < nhalos; i++) g->halos[i] = halos[i];
+  g->instance = &rt().inst;
+  g->index = (int)rt().groups.size();
+  rt().groups.push_back(g);
+  rt().groupx.push_back(GroupX());
+  return g;
+}
+
+static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
+  std::vector<ob2_halo_task> tasks;
+  gx.key.clear();
+  gx.max_pts = 0;
+  for (int hh = 0; hh < g->nhalos; hh++) {
+    ops_halo h = g->halos[hh];
+    for (int i = 3; i < OPS_MAX_DIM; i++)
+      if (h->iter_size[i] != 1)
+        throw OPSException(OPS_NOT_IMPLEMENTED, "Error: halos above 3D are not supported");
+    if (h->from->dim != h->to->dim)
+      throw OPSException(OPS_INVALID_ARGUMENT,
+                         "Error: ops_halo_transfer between dats of different dim");
+    ob2_halo_task t;
+    memset(&t, 0, sizeof(t));
+    t.src = h->from->data_d;
+    t.dst = h->to->data_d;
+    t.src_type = h->from->type_size;
+    t.dst_type = h->to->type_size;
+    if (t.src_type != t.dst_type) {
+      bool okf = (!strcmp(h->from->type, "double") || !strcmp(h->from->type, "float")) &&
+                 (!strcmp(h->to->type, "double") || !strcmp(h->to->type, "float"));
+      if (!okf)
+        throw OPSException(OPS_NOT_IMPLEMENTED, "Error: unsupported mixed-type halo transfer");
+      t.float_kind = 1;
+    }
+    t.ncomp = h->from->dim;
+    t.src_soa = t.dst_soa = rt().inst.OPS_soa;
+    t.npts = 1;
+    for (int a = 0; a < 3; a++) {
+      t.iter[a] = h->iter_size[a];
+      t.npts *= h->iter_size[a];
+    }
+    long long fc = 1, tc = 1;
+    for (int i = 0; i < 3; i++) {
+      t.src_axis[i] = abs(h->from_dir[i]) - 1;
+      t.src_flip[i] = h->from_dir[i] < 0;
+      t.src_start[i] = h->from_base[i] - h->from->d_m[i] - h->from->base[i];
+      t.src_cum[i] = fc;
+      fc *= h->from->size[i];
+      t.dst_axis[i] = abs(h->to_dir[i]) - 1;
+      t.dst_flip[i] = h->to_dir[i] < 0;
+      t.dst_start[i] = h->to_base[i] - h->to->d_m[i] - h->to->base[i];
+      t.dst_cum[i] = tc;
+      tc *= h->to->size[i];
+      if (t.src_axis[i] < 0 || t.src_axis[i] > 2 || t.dst_axis[i] < 0 || t.dst_axis[i] > 2)
+        throw OPSException(OPS_INVALID_ARGUMENT, "Error: invalid halo direction");
+    }
+    t.src_npts_total = fc;
+    t.dst_npts_total = tc;
+    // bounds: every touched storage index must lie inside the dats
+    for (int i = 0; i < 3; i++) {
+      int fl = t.iter[t.src_axis[i]], tl = t.iter[t.dst_axis[i]];
+      if (t.src_start[i] < 0 || t.src_start[i] + fl > h->from->size[i] || t.dst_start[i] < 0 ||
+          t.dst_start[i] + tl > h->to->size[i]) {
+        OPSException ex(OPS_INVALID_ARGUMENT);
+        ex << "Error: halo " << hh << " of group " << g->index << " reaches outside dat "
+           << h->from->name << " or " << h->to->name;
+        throw ex;
+      }
+    }
+    if (t.npts > gx.max_pts) gx.max_pts = t.npts;
+    tasks.push_back(t);
+    gx.key.push_back(h->from->data_d);
+    gx.key.push_back(h->to->data_d);
+  }
+  if (gx.tasks_d) {
+    ob2_dev_sync();
+    ob2_dev_free(gx.tasks_d);
+    gx.tasks_d = nullptr;
+  }
+  gx.ntasks = (int)tasks.size();
+  if (gx.ntasks) {
+    size_t bytes = sizeof(ob2_halo_task) * tasks.size();
+    check(ob2_dev_malloc(&gx.tasks_d, bytes), "ops_halo_transfer");
+    check(ob2_dev_h2d(gx.tasks_d, tasks.data(), bytes), "ops_halo_transfer");
+  }
+}
+
+OPS_API void ops_halo_transfer(ops_halo_group g) {
+  require_init();
+  GroupX &gx = rt().groupx[g->index];
+  bool stale = gx.ntasks != g->nhalos || gx.key.size() != (size_t)2 * g->nhalos;
+  for (int hh = 0; !stale && hh < g->nhalos; hh++)
+    stale = gx.key[2 * hh] != g->halos[hh]->from->data_d ||
+            gx.key[2 * hh + 1] != g->halos[hh]->to->data_d;
+  if (stale) build_halo_tasks(g, gx);
+  for (int hh = 0; hh < g->nhalos; hh++) {
+    put_data(g->halos[hh]->from);
+    put_data(g->halos[hh]->to);
+  }
+  int k = kernel_slot("ops_halo_transfer");
+  double t0 = wall();
+  check(ob2_halo_run((const ob2_halo_task *)gx.tasks_d, gx.ntasks, gx.max_pts),
+        "ops_halo_transfer");
+  KStat &s = rt().kstats[k];
+  s.count++;
+  s.host_s += wall() - t0;
+  for (int hh = 0; hh < g->nhalos; hh++) {
+    ops_halo h = g->halos[hh];
+    h->to->dirty_hd = 2;
+    s.transfer += 2.0 * (double)h->from->elem_size * h->iter_size[0] * h->iter_size[1] *
+                  h->iter_size[2];
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * constants (ops_decl_const_char: cudaMemcpyToSymbol in the reference,
+ * master_kernel.cpp.j2:40-70).  The generated kernels file registers the
+ * copier for its __constant__ symbols.
+ * ---------------------------------------------------------------------- */
+OPS_API void ob2_register_const_handler(ob2_const_fn fn) { rt().const_fn = fn; }
+
+OPS_API void ops_decl_const_char(OPS_instance *, int dim, char const *, int type_size, char *data,
+                                 char const *name) {
+  require_init();
+  if (!rt().const_fn) return;  // no generated kernel uses constants
+  int rc = rt().const_fn(name, dim, type_size, data, ob2_dev_stream());
+  if (rc < 0) {
+    OPSException ex(OPS_INVALID_ARGUMENT);
+    ex << "Error: ops_decl_const " << name << " larger than its device symbol";
+    throw ex;
+  }
+  check(rc, "ops_decl_const");
+}
+
+/* all work is stream ordered: nothing is queued host-side */
+OPS_API void ops_execute(OPS_instance *) {}
+
+/* ------------------------------------------------------------------------
+ * par_loop support for generated stubs (loop_host.cpp.j2:13-780)
+ * ---------------------------------------------------------------------- */
+OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int dim,
+                           const int *range, ops_arg *args, int nargs) {
+  require_init();
+  Runtime &r = rt();
+  if (nargs > OB2_MAX_ARGS)
+    throw OPSException(OPS_NOT_IMPLEMENTED, "Error: too many arguments in ops_par_loop");
+  L->name = name;
+  L->dim = dim;
+  L->nargs = nargs;
+  L->args = args;
+  L->stream = ob2_dev_stream();
+  L->npoints = 1;
+  for (int i = 0; i < 3; i++) {
+    L->lo[i] = i < dim ? range[2 * i] : 0;
+    L->hi[i] = i < dim ? range[2 * i + 1] : 1;
+    L->n[i] = std::max(0, L->hi[i] - L->lo[i]);
+    L->npoints *= L->n[i];
+  }
+  L->kernel_index = kernel_slot(name);
+  L->block[0] = r.block_x;
+  L->block[1] = dim > 1 ? r.block_y : 1;
+  L->block[2] = dim > 2 ? r.block_z : 1;
+  L->host_t0 = wall();
+  L->ev_start = L->ev_end = nullptr;
+  if (L->npoints == 0) return 0;
+
+  size_t red_bytes = 0;
+  int nred = 0;
+  const int soa = r.inst.OPS_soa;
+  for (int i = 0; i < nargs; i++) {
+    ops_arg &a = args[i];
+    ob2_view &v = L->view[i];
+    memset(&v, 0, sizeof(v));
+    L->red[i].acc = nullptr;
+    L->red[i].first = 0;
+    L->red[i].op = 0;
+    if (a.argtype == OPS_ARG_DAT) {
+      if (!a.opt || !a.dat) continue;
+      ops_dat d = a.dat;
+      if (d->locked_hd) {
+        OPSException ex(OPS_INVALID_ARGUMENT);
+        ex << "Error: ops_par_loop " << name << " called with dat " << d->name
+           << " whose raw pointer was not released";
+        throw ex;
+      }
+      put_data(d);
+      // low-dim accumulation: first INC/MIN/MAX since another access fills
+      // the dat with the identity (ops_dummy_singlenode.cpp:235-391)
+      DatX &dx = r.datx[d->index];
+      if (d->e_dat && (a.acc == OPS_INC || a.acc == OPS_MIN || a.acc == OPS_MAX) &&
+          dx.edat_prev_acc != a.acc) {
+        dx.edat_prev_acc = a.acc;
+        unsigned char idv[8];
+        int tc = type_code(d->type);
+        identity_bytes(tc, a.acc, idv, true);
+        check(ob2_fill_value(d->data_d, idv, d->type_size, d->mem / d->type_size),
+              "low-dim init");
+      }
+      if (d->block->dims != block->dims && !d->e_dat) {
+        // dats of other blocks are allowed as long as the dims agree
+      }
+      const int md = d->dim;
+      const int *st = a.stencil ? a.stencil->stride : nullptr;
+      long long cum = 1, off = 0;
+      long long step[3] = {0, 0, 0};
+      for (int k = 0; k < block->dims && k < 3; k++) {
+        int sk = st ? st[k] : 1;
+        off += cum * (long long)(-d->base[k] - d->d_m[k]);
+        step[k] = cum * sk;
+        cum *= d->size[k];
+      }
+      if (soa) {
+        v.ex = 1;
+        v.ey = d->size[0];
+        v.ez = d->size[0] * d->size[1];
+        v.ed = (int)cum;
+        v.base = d->data_d + off * d->type_size;
+        v.wx = step[0];
+        v.wy = step[1];
+        v.wz = step[2];
+      } else {
+        v.ex = md;
+        v.ey = d->size[0] * md;
+        v.ez = d->size[0] * d->size[1] * md;
+        v.ed = 1;
+        v.base = d->data_d + off * d->elem_size;
+        v.wx = step[0] * md;
+        v.wy = step[1] * md;
+        v.wz = step[2] * md;
+      }
+    } else if (a.argtype == OPS_ARG_GBL && a.acc != OPS_READ) {
+      ops_reduction h = (ops_reduction)a.data;
+      RedX &x = r.redx[h->index];
+      if (!h->initialized) {
+        OPSException ex(OPS_INVALID_ARGUMENT);
+        ex << "Error: reduction handle " << h->name << " used without ops_arg_reduce";
+        throw ex;
+      }
+      L->red[i].acc = x.acc_d;
+      L->red[i].first = x.pending_first;
+      L->red[i].op = a.acc;
+      x.pending_first = 0;
+      red_bytes += (size_t)h->size;
+      nred++;
+    }
+  }
+  // scratch for per-CTA partials (grid = ceil(n/block) per axis); each
+  // reduction argument's region is rounded up to 256 bytes by the stub
+  long long nblk = 1;
+  for (int i = 0; i < 3; i++) nblk *= (L->n[i] + L->block[i] - 1) / L->block[i];
+  size_t need = red_bytes * (size_t)nblk + 256 * (size_t)nred;
+  if (need > r.partials_cap) {
+    if (r.partials) {
+      ob2_dev_sync();
+      ob2_dev_free(r.partials);
+    }
+    size_t cap = std::max(need, (size_t)1 << 20);
+    check(ob2_dev_malloc(&r.partials, cap), "reduction scratch");
+    r.partials_cap = cap;
+  }
+  L->partials = r.partials;
+  L->partials_bytes = r.partials_cap;
+  L->counter = r.counter;
+  if (r.inst.OPS_diags > 1) {
+    ob2_event_create(&L->ev_start);
+    ob2_event_create(&L->ev_end);
+    ob2_event_record(L->ev_start);
+  }
+  return 1;
+}
+
+OPS_API void ob2_loop_check_launch(ob2_loop *L) {
+  int e = ob2_last_launch_error();
+  if (e) {
+    OPSException ex(OPS_RUNTIME_ERROR);
+    ex << "Error: kernel launch of ops_par_loop " << L->name << " failed: " << ob2_error_string(e);
+    throw ex;
+  }
+}
+
+OPS_API void ob2_loop_end(ob2_loop *L) {
+  Runtime &r = rt();
+  KStat &s = r.kstats[L->kernel_index];
+  s.count++;
+  if (L->ev_start) {
+    ob2_event_record(L->ev_end);
+    float ms = 0.f;
+    check(ob2_event_elapsed_ms(L->ev_start, L->ev_end, &ms), L->name);
+    s.dev_ms += ms;
+    ob2_event_destroy(L->ev_start);
+    ob2_event_destroy(L->ev_end);
+    L->ev_start = L->ev_end = nullptr;
+  }
+  s.host_s += wall() - L->host_t0;
+  for (int i = 0; i < L->nargs; i++) {
+    ops_arg &a = L->args[i];
+    if (a.argtype != OPS_ARG_DAT || !a.opt || !a.dat) continue;
+    ops_dat d = a.dat;
+    if (a.acc != OPS_READ) d->dirty_hd = 2;
+    if (d->e_dat && (a.acc == OPS_READ || a.acc == OPS_WRITE || a.acc == OPS_RW))
+      r.datx[d->index].edat_prev_acc = a.acc;
+    // transfer model (ops_lib_core.cpp:1687-1697)
+    s.transfer += (double)L->npoints * d->elem_size *
+                  ((a.acc == OPS_RW || a.acc == OPS_INC) ? 2.0 : 1.0);
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * output / timing (ops_lib_core.cpp:1468-1647)
+ * ---------------------------------------------------------------------- */
+OPS_API void ops_printf(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vprintf(fmt, ap);
+  va_end(ap);
+}
+OPS_API void ops_fprintf(FILE *f, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vfprintf(f, fmt, ap);
+  va_end(ap);
+}
+OPS_API void ops_diagnostic_output(void) {
+  Runtime &r = rt();
+  if (r.inst.OPS_diags <= 1) return;
+  printf("\n OPS diagnostic output (B200 backend)\n --------------------------------\n");
+  printf(" blocks %zu, dats %zu, stencils %zu, halos %zu\n", r.blocks.size(), r.dats.size(),
+         r.stencils.size(), r.halos.size());
+  size_t tot = 0;
+  for (ops_dat d : r.dats)
+    if (d) tot += d->mem;
+  printf(" total device memory in dats: %.3f MB\n", tot / 1e6);
+}
+OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
+  Runtime &r = rt();
+  ob2_dev_sync();
+  std::string s;
+  char line[320];
+  snprintf(line, sizeof line, "\n  %-40s %8s %14s %14s %10s\n", "Timings (B200 backend)", "count",
+           "time(s)", "device(ms)", "GB/s");
+  s += line;
+  double tt = 0.0;
+  for (auto &k : r.kstats) {
+    double t = k.dev_ms > 0 ? k.dev_ms * 1e-3 : k.host_s;
+    tt += k.host_s;
+    snprintf(line, sizeof line, "  %-40s %8ld %14.6f %14.4f %10.2f\n", k.name.c_str(), k.count,
+             k.host_s, k.dev_ms, t > 0 ? k.transfer / t / 1e9 : 0.0);
+    s += line;
+  }
+  snprintf(line, sizeof line, "  Total kernel time (host): %f\n", tt);
+  s += line;
+  if (buf && n) {
+    size_t m = std::min(n - 1, s.size());
+    memcpy(buf, s.data(), m);
+    buf[m] = 0;
+  }
+  return s.size();
+}
+OPS_API void ops_timing_output_stdout(void) {
+  size_t n = ops_timing_output_str(nullptr, 0);
+  std::string s(n + 1, 0);
+  ops_timing_output_str(&s[0], n + 1);
+  fputs(s.c_str(), stdout);
+}
+OPS_API void ops_timers_core(double *cpu, double *et) {
+  *cpu = (double)clock() / CLOCKS_PER_SEC;
+  *et = wall();
+}
+/* like the reference CUDA backend's ops_timers: device work is complete at
+ * the returned time stamp */
+OPS_API void ops_timers(double *cpu, double *et) {
+  if (R && R->initialised) ob2_dev_sync();
+  ops_timers_core(cpu, et);
+}
+OPS_API int ops_is_root(void) { return 1; }
+OPS_API void ops_partition(const char *) {}
+OPS_API void ops_partition_opts_c(const char *) {}
+OPS_API void ops_get_data(ops_dat d) { get_data(d); }
+OPS_API void ops_put_data(ops_dat d) { put_data(d); }
+OPS_API bool ops_checkpointing_init(const char *, double, int) { return false; }
+OPS_API void ops_checkpointing_initphase_done(void) {}
+OPS_API void ops_reset_gpu_power_counters(void) {}
+OPS_API double ops_get_gpu_energy_consumed(void) { return 0.0; }
+OPS_API void *xmalloc(size_t n) {
+  void *p = malloc(n);
+  if (!p && n) throw OPSException(OPS_RUNTIME_ERROR, "Error: xmalloc failed");
+  return p;
+}
+OPS_API void *xrealloc(void *p, size_t n) {
+  void *q = realloc(p, n);
+  if (!q && n) throw OPSException(OPS_RUNTIME_ERROR, "Error: xrealloc failed");
+  return q;
+}
+OPS_API void *xcalloc(size_t k, size_t n) {
+  void *p = calloc(k, n);
+  if (!p && k != 0 && n != 0) throw OPSException(OPS_RUNTIME_ERROR, "Error: xcalloc failed");
+  return p;
+}
+
+OPS_API void ops_print_dat_to_txtfile(ops_dat d, const char *file) {
+  get_data(d);
+  FILE *f = fopen(file, "a");
+  if (!f) return;
+  fprintf(f, "ops_dat %s, dim %d, sizes %d %d %d\n", d->name, d->dim, d->size[0], d->size[1],
+          d->size[2]);
+  size_t n = dat_points(d) * d->dim;
+  for (size_t i = 0; i < n; i++) {
+    if (!strcmp(d->type, "double"))
+      fprintf(f, " %3.10lf", ((double *)d->data)[i]);
+    else if (!strcmp(d->type, "float"))
+      fprintf(f, " %3.10f", ((float *)d->data)[i]);
+    else if (!strcmp(d->type, "int"))
+      fprintf(f, " %d", ((int *)d->data)[i]);
+    if ((i + 1) % (size_t)(d->size[0] * d->dim) == 0) fprintf(f, "\n");
+  }
+  fclose(f);
+}
+OPS_API void ops_print_dat_to_txtfile_core(ops_dat d, const char *file) {
+  ops_print_dat_to_txtfile(d, file);
+}
+
+/* ------------------------------------------------------------------------
+ * external access (ops_dummy_singlenode.cpp:630-850)
+ * ---------------------------------------------------------------------- */
+OPS_API int ops_dat_get_local_npartitions(ops_dat) { return 1; }
+OPS_API int ops_dat_get_global_npartitions(ops_dat) { return 1; }
+OPS_API void ops_dat_get_extents(ops_dat d, int, int *disp, int *size) {
+  for (int i = 0; i < d->block->dims; i++) {
+    if (disp) disp[i] = 0;
+    if (size) size[i] = d->size[i] + d->d_m[i] - d->d_p[i];
+  }
+}
+OPS_API size_t ops_dat_get_slab_extents(ops_dat d, int part, int *disp, int *size, int *slab) {
+  int ext[OPS_MAX_DIM];
+  ops_dat_get_extents(d, part, nullptr, ext);
+  size_t bytes = d->elem_size;
+  for (int i = 0; i < d->block->dims; i++) {
+    if (slab[2 * i] < 0 || slab[2 * i + 1] > ext[i]) {
+      OPSException ex(OPS_RUNTIME_ERROR);
+      ex << "Error: ops_dat_get_slab_extents() called on " << d->name
+         << " with slab ranges in dimension " << i << ": " << slab[2 * i] << "-"
+         << slab[2 * i + 1] << " beyond data size 0-" << ext[i];
+      throw ex;
+    }
+    disp[i] = slab[2 * i];
+    size[i] = slab[2 * i + 1] - slab[2 * i];
+    bytes *= size[i];
+  }
+  return bytes;
+}
+OPS_API void ops_dat_get_raw_metadata(ops_dat d, int part, int *disp, int *size, int *stride,
+                                      int *d_m, int *d_p) {
+  ops_dat_get_extents(d, part, disp, size);
+  for (int i = 0; i < d->block->dims; i++) {
+    if (stride) stride[i] = d->size[i];
+    if (d_m) d_m[i] = d->d_m[i];
+    if (d_p) d_p[i] = d->d_p[i];
+  }
+}
+/* ops_dummy_singlenode.cpp:662-707 */
+OPS_API char *ops_dat_get_raw_pointer(ops_dat d, int, ops_stencil, ops_memspace *ms) {
+  require_init();
+  if (ms && *ms == OPS_HOST) {
+    get_data(d);
+    d->locked_hd = OPS_HOST;
+    return d->data + d->base_offset;
+  }
+  put_data(d);
+  if (ms) *ms = OPS_DEVICE;
+  d->locked_hd = OPS_DEVICE;
+  return d->data_d + d->base_offset;
+}
+/* ops_dummy_singlenode.cpp:709-735 */
+OPS_API void ops_dat_release_raw_data(ops_dat d, int, ops_access acc) {
+  if (!d->locked_hd) {
+    OPSException ex(OPS_RUNTIME_ERROR);
+    ex << "Error: ops_dat_release_raw_data() called, but with no matching "
+          "ops_dat_get_raw_pointer() beforehand: "
+       << d->name;
+    throw ex;
+  }
+  if (acc != OPS_READ) d->dirty_hd = d->locked_hd == OPS_HOST ? 1 : 2;
+  d->locked_hd = 0;
+}
+OPS_API void ops_dat_release_raw_data_memspace(ops_dat d, int part, ops_access acc,
+                                               ops_memspace *ms) {
+  if (ms && d->locked_hd) d->locked_hd = *ms;
+  ops_dat_release_raw_data(d, part, acc);
+}
+
+static void stage_reserve(size_t n) {
+  Runtime &r = rt();
+  if (n > r.stage_cap) {
+    if (r.stage_d) {
+      ob2_dev_sync();
+      ob2_dev_free(r.stage_d);
+    }
+    check(ob2_dev_malloc((void **)&r.stage_d, n), "staging buffer");
+    r.stage_cap = n;
+  }
+}
+
+/* packed AoS slab <-> dat: dir 0 fetch, 1 set (ops_util.cpp:353-500) */
+static void slab_io(ops_dat d, char *data, const int *range, ops_memspace ms, int dir) {
+  require_init();
+  int start[3] = {0, 0, 0}, count[3] = {1, 1, 1}, size3[3] = {1, 1, 1};
+  size_t pts = 1;
+  for (int i = 0; i < 3; i++) size3[i] = d->size[i];
+  for (int i = 0; i < d->block->dims && i < 3; i++) {
+    start[i] = range[2 * i] - d->d_m[i];
+    count[i] = range[2 * i + 1] - range[2 * i];
+    if (count[i] < 0 || start[i] < 0 || start[i] + count[i] > d->size[i])
+      throw OPSException(OPS_RUNTIME_ERROR, "Error: slab range outside the dat");
+    pts *= (size_t)count[i];
+  }
+  size_t bytes = pts * d->elem_size;
+  if (bytes == 0) return;
+  put_data(d);
+  char *buf = data;
+  if (ms != OPS_DEVICE) {
+    stage_reserve(bytes);
+    buf = rt().stage_d;
+    if (dir == 1) check(ob2_dev_h2d(buf, data, bytes), "ops_dat_set_data");
+  }
+  check(ob2_box_copy(d->data_d, d->type_size, d->dim, rt().inst.OPS_soa, size3, start, count,
+                     buf, dir),
+        dir == 0 ? "ops_dat_fetch_data" : "ops_dat_set_data");
+  if (ms != OPS_DEVICE && dir == 0) check(ob2_dev_d2h(data, buf, bytes), "ops_dat_fetch_data");
+  if (ms == OPS_DEVICE) check(ob2_dev_sync(), "slab copy");
+  if (dir == 1) d->dirty_hd = 2;
+}
+static void full_range(ops_dat d, int *r) {
+  int ext[OPS_MAX_DIM];
+  ops_dat_get_extents(d, 0, nullptr, ext);
+  for (int i = 0; i < OPS_MAX_DIM; i++) {
+    r[2 * i] = 0;
+    r[2 * i + 1] = i < d->block->dims ? ext[i] : 1;
+  }
+}
+OPS_API void ops_dat_fetch_data_memspace(ops_dat d, int, char *data, ops_memspace ms) {
+  int r[2 * OPS_MAX_DIM];
+  full_range(d, r);
+  slab_io(d, data, r, ms, 0);
+}
+OPS_API void ops_dat_fetch_data(ops_dat d, int part, char *data) {
+  ops_dat_fetch_data_memspace(d, part, data, OPS_HOST);
+}
+OPS_API void ops_dat_fetch_data_slab_memspace(ops_dat d, int, char *data, int *range,
+                                              ops_memspace ms) {
+  slab_io(d, data, range, ms, 0);
+}
+OPS_API void ops_dat_set_data_memspace(ops_dat d, int, char *data, ops_memspace ms) {
+  int r[2 * OPS_MAX_DIM];
+  full_range(d, r);
+  slab_io(d, data, r, ms, 1);
+}
+OPS_API void ops_dat_set_data(ops_dat d, int part, char *data) {
+  ops_dat_set_data_memspace(d, part, data, OPS_HOST);
+}
+OPS_API void ops_dat_set_data_slab_memspace(ops_dat d, int, char *data, int *range,
+                                            ops_memspace ms) {
+  slab_io(d, data, range, ms, 1);
+}
+
+/* ------------------------------------------------------------------------
+ * random fills: counter-based stream generated on the device
+ * (replaces cuRAND in ops_cuda_common.cu:184-283)
+ * ---------------------------------------------------------------------- */
+OPS_API void ops_randomgen_init(unsigned int seed, int) {
+  rt().rng_seed = seed;
+  rt().rng_counter = 0;
+}
+OPS_API void ops_randomgen_exit(void) {}
+static void fill_rand(ops_dat d, int normal) {
+  require_init();
+  if (d->type_size != 8 && d->type_size != 4)
+    throw OPSException(OPS_NOT_IMPLEMENTED, "Error: random fill needs a float or double dat");
+  size_t n = dat_points(d) * d->dim;
+  check(ob2_fill_random(d->data_d, d->type_size, n, rt().rng_seed, rt().rng_counter, normal),
+        "ops_fill_random");
+  rt().rng_counter += n;
+  d->dirty_hd = 2;
+}
+OPS_API void ops_fill_random_uniform(ops_dat d) { fill_rand(d, 0); }
+OPS_API void ops_fill_random_normal(ops_dat d) { fill_rand(d, 1); }
+
+/* ------------------------------------------------------------------------
+ * tridiagonal (ops_tridiag_cuda.cpp:96-251: size/type checks, raw pointers
+ * at the range origin, solve along solvedim)
+ * ---------------------------------------------------------------------- */
+static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_dat c, ops_dat d,
+                 ops_dat u) {
+  require_init();
+  if (ndim < 1 || ndim > 3 || solvedim < 0 || solvedim >= ndim)
+    throw OPSException(OPS_INVALID_ARGUMENT, "Tridsolver error: bad ndim or solvedim");
+  for (int i = 0; i < ndim; i++)
+    if (a->size[i] != b->size[i] || b->size[i] != c->size[i] || c->size[i] != d->size[i] ||
+        (u && u->size[i] != d->size[i]))
+      throw OPSException(OPS_RUNTIME_ERROR,
+                         "Tridsolver error: the a,b,c,d datasets all need to be the same size");
+  if (strcmp(a->type, b->type) || strcmp(b->type, c->type) || strcmp(c->type, d->type) ||
+      (u && strcmp(d->type, u->type)))
+    throw OPSException(OPS_RUNTIME_ERROR,
+                       "Tridsolver error: the a,b,c,d datasets must all be of the same type");
+  if (strcmp(a->type, "double") && strcmp(a->type, "float"))
+    throw OPSException(OPS_RUNTIME_ERROR,
+                       "Tridsolver error: unsupported type. Dataset type must either be "
+                       "\"double\" or \"float\"");
+  ops_dat all[5] = {a, b, c, d, u};
+  for (int i = 0; i < 5; i++)
+    if (all[i]) {
+      if (all[i]->locked_hd)
+        throw OPSException(OPS_INVALID_ARGUMENT, "Tridsolver error: dat raw pointer not released");
+      put_data(all[i]);
+    }
+  int dims[3] = {1, 1, 1};
+  long long strides[3] = {1, a->size[0], (long long)a->size[0] * a->size[1]};
+  long long off = 0;
+  for (int i = 0; i < ndim; i++) {
+    dims[i] = range[2 * i + 1] - range[2 * i];
+    long long s0 = (long long)range[2 * i] - a->d_m[i] - a->base[i];
+    if (dims[i] < 0 || s0 < 0 || s0 + dims[i] > a->size[i])
+      throw OPSException(OPS_INVALID_ARGUMENT, "Tridsolver error: range outside the datasets");
+    off += s0 * strides[i];
+  }
+  size_t ts = a->type_size;
+  int k = kernel_slot(u ? "ops_tridMultiDimBatch_Inc" : "ops_tridMultiDimBatch");
+  double t0 = wall();
+  int rc = ob2_trid_batch((int)ts, ndim, solvedim, dims, strides, a->data_d + off * ts,
+                          b->data_d + off * ts, c->data_d + off * ts, d->data_d + off * ts,
+                          u ? u->data_d + off * ts : nullptr);
+  if (rc) {
+    OPSException ex(OPS_RUNTIME_ERROR);
+    ex << "Tridsolver error: " << ob2_error_string(rc) << " (line length "
+       << dims[solvedim] << ", max 4096)";
+    throw ex;
+  }
+  KStat &s = rt().kstats[k];
+  s.count++;
+  s.host_s += wall() - t0;
+  double pts = (double)dims[0] * dims[1] * dims[2];
+  s.transfer += pts * ts * (u ? 6.0 : 5.0);
+  (u ? u : d)->dirty_hd = 2;
+}
+OPS_API void ops_tridMultiDimBatch(int ndim, int solvedim, int *range, ops_dat a, ops_dat b,
+                                   ops_dat c, ops_dat d, ops_tridsolver_params *) {
+  trid(ndim, solvedim, range, a, b, c, d, nullptr);
+}
+OPS_API void ops_tridMultiDimBatch_Inc(int ndim, int solvedim, int *range, ops_dat a,
+                                       ops_dat b, ops_dat c, ops_dat d, ops_dat u,
+                                       ops_tridsolver_params *) {
+  trid(ndim, solvedim, range, a, b, c, d, u);
+}
+
+/* ------------------------------------------------------------------------
+ * dump hook (same format as the oracle): every live dat, halos included
+ * ---------------------------------------------------------------------- */
+OPS_API void ops_dump_dats(const char *path) {
+  FILE *f = fopen(path, "wb");
+  if (!f) return;
+  for (ops_dat d : rt().dats) {
+    if (!d) continue;
+    get_data(d);
+    int nl = (int)strlen(d->name);
+    fwrite("DAT0", 1, 4, f);
+    fwrite(&nl, 4, 1, f);
+    fwrite(d->name, 1, nl, f);
+    int tl = (int)strlen(d->type);
+    fwrite(&tl, 4, 1, f);
+    fwrite(d->type, 1, tl, f);
+    int meta[4] = {d->dim, d->type_size, d->block->dims, rt().inst.OPS_soa};
+    fwrite(meta, 4, 4, f);
+    fwrite(d->size, 4, OPS_MAX_DIM, f);
+    fwrite(d->d_m, 4, OPS_MAX_DIM, f);
+    fwrite(d->d_p, 4, OPS_MAX_DIM, f);
+    unsigned long long nb = d->mem;
+    fwrite(&nb, 8, 1, f);
+    fwrite(d->data, 1, d->mem, f);
+  }
+  fclose(f);
+}

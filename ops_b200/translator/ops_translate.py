@@ -1,0 +1,658 @@
+"""Source-to-source translator: OPS application -> B200 (sm_100a) build.
+
+Plays the role of the reference's code generators
+(ops_translator/ops-translator/ with the templates in
+ops_translator/resources/templates/cpp/cuda/loop_host.cpp.j2, and the legacy
+ops_translator_legacy/c/ops_gen_mpi_cuda.py): every ``ops_par_loop`` call site
+is rewritten into a call of a generated host stub, and every distinct loop gets
+one hand-written-style CUDA kernel.  The parser is this project's own (a small
+comment/string-aware scanner; libclang is not needed).
+
+Output for an application made of sources S1.cpp ... Sn.cpp:
+  * ``S_ops.cpp`` per source: the source with ``ops_seq_v2.h`` replaced by the
+    backend headers plus stub prototypes, and ``ops_par_loop(k, ...)`` replaced
+    by ``ops_par_loop_<k>(...)``;
+  * ``<app>_kernels.cu``: all user kernels (copied verbatim as __device__
+    functions), every ``ops_decl_const`` as a __constant__ symbol, one
+    __global__ kernel and one host stub per loop, and the constant copier.
+
+Kernel shape (per loop): one thread per grid point; x on threadIdx.x so that
+every dat access of a warp is one contiguous run along x; CTA shape from the
+runtime (OPS_BLOCK_SIZE_X/Y/Z, default 32x4x1); ops_arg_gbl(READ) values are
+passed by value inside the kernel parameters (copied at call time, the
+reference's lazy semantics, ops_lazy.cpp:1433-1437); reductions go through
+the warp-shuffle / last-CTA combine of include/ops_b200_kernel.h.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import sys
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+# --------------------------------------------------------------------------
+# scanning helpers
+# --------------------------------------------------------------------------
+
+
+def mask_comments_strings(src: str, keep_strings: bool = False) -> str:
+    """Return src with comments (and, unless keep_strings, string/char
+    literal contents) replaced by spaces; offsets and newlines preserved."""
+    out = list(src)
+    i, n = 0, len(src)
+    while i < n:
+        c = src[i]
+        if c == "/" and i + 1 < n and src[i + 1] == "/":
+            j = src.find("\n", i)
+            j = n if j < 0 else j
+            for k in range(i, j):
+                out[k] = " "
+            i = j
+        elif c == "/" and i + 1 < n and src[i + 1] == "*":
+            j = src.find("*/", i + 2)
+            j = n if j < 0 else j + 2
+            for k in range(i, j):
+                if src[k] != "\n":
+                    out[k] = " "
+            i = j
+        elif c in "\"'":
+            q = c
+            j = i + 1
+            while j < n and src[j] != q:
+                if src[j] == "\\":
+                    j += 1
+                j += 1
+            if not keep_strings:
+                for k in range(i + 1, min(j, n)):
+                    if src[k] != "\n":
+                        out[k] = " "
+            i = j + 1
+        else:
+            i += 1
+    return "".join(out)
+
+
+def match_paren(masked: str, open_idx: int) -> int:
+    """Index of the bracket closing the one at open_idx (in masked text)."""
+    pairs = {"(": ")", "{": "}", "[": "]"}
+    opener = masked[open_idx]
+    closer = pairs[opener]
+    depth = 0
+    for i in range(open_idx, len(masked)):
+        ch = masked[i]
+        if ch == opener:
+            depth += 1
+        elif ch == closer:
+            depth -= 1
+            if depth == 0:
+                return i
+    raise ValueError("unbalanced bracket at offset %d" % open_idx)
+
+
+def split_top(text: str, masked: str) -> List[str]:
+    """Split text at top-level commas (masked guides the nesting)."""
+    parts, depth, start = [], 0, 0
+    for i, ch in enumerate(masked):
+        if ch in "([{":
+            depth += 1
+        elif ch in ")]}":
+            depth -= 1
+        elif ch == "," and depth == 0:
+            parts.append(text[start:i].strip())
+            start = i + 1
+    tail = text[start:].strip()
+    if tail or parts:
+        parts.append(tail)
+    return parts
+
+
+def find_calls(src: str, name: str) -> List[Tuple[int, int, List[str]]]:
+    """All calls `name(...)`: (start, end_exclusive, args)."""
+    masked = mask_comments_strings(src)
+    res = []
+    for m in re.finditer(r"(?<![\w.>])" + re.escape(name) + r"\s*\(", masked):
+        op = m.end() - 1
+        cl = match_paren(masked, op)
+        args = split_top(src[op + 1:cl], masked[op + 1:cl])
+        res.append((m.start(), cl + 1, args))
+    return res
+
+
+def unquote(s: str) -> str:
+    s = s.strip()
+    if len(s) >= 2 and s[0] == '"' and s[-1] == '"':
+        return s[1:-1]
+    return s
+
+
+# --------------------------------------------------------------------------
+# model
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class LoopArg:
+    kind: str  # dat | gbl | reduce | idx
+    ctype: str = ""  # element type string
+    dim: str = "1"  # dimension expression
+    acc: str = "OPS_READ"
+    opt: bool = False
+
+    def key(self) -> Tuple:
+        return (self.kind, self.ctype, self.dim if self.kind != "dat" else
+                ("1" if self.dim.strip() == "1" else "n"), self.acc, self.opt)
+
+
+@dataclass
+class KernelParam:
+    text: str
+    base_type: str  # e.g. double
+    is_acc: bool
+    is_const: bool
+    name: str
+
+
+@dataclass
+class KernelDef:
+    name: str
+    params: List[KernelParam]
+    text: str  # full definition text
+    header: str  # file it came from
+
+
+@dataclass
+class Loop:
+    kernel: str
+    ndim: int
+    args: List[LoopArg]
+    stub: str = ""
+    sources: List[str] = field(default_factory=list)
+
+    def key(self) -> Tuple:
+        return (self.kernel, self.ndim, tuple(a.key() for a in self.args))
+
+
+@dataclass
+class ConstDecl:
+    name: str
+    dim: str
+    ctype: str
+
+
+ACCESS = {"OPS_READ", "OPS_WRITE", "OPS_RW", "OPS_INC", "OPS_MIN", "OPS_MAX"}
+
+
+def parse_arg(text: str, where: str) -> LoopArg:
+    masked = mask_comments_strings(text)
+    m = re.match(r"\s*(ops_arg_\w+)\s*\(", masked)
+    if not m:
+        raise SystemExit("%s: cannot parse ops_par_loop argument: %s" % (where, text))
+    fn = m.group(1)
+    op = m.end() - 1
+    cl = match_paren(masked, op)
+    inner = split_top(text[op + 1:cl], masked[op + 1:cl])
+    if fn == "ops_arg_dat":
+        if len(inner) != 5:
+            raise SystemExit("%s: ops_arg_dat needs 5 arguments: %s" % (where, text))
+        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip())
+    if fn == "ops_arg_dat_opt":
+        if len(inner) != 6:
+            raise SystemExit("%s: ops_arg_dat_opt needs 6 arguments: %s" % (where, text))
+        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip(), opt=True)
+    if fn == "ops_arg_gbl":
+        if len(inner) != 4:
+            raise SystemExit("%s: ops_arg_gbl needs 4 arguments: %s" % (where, text))
+        acc = inner[3].strip()
+        if acc != "OPS_READ":
+            raise SystemExit("%s: ops_arg_gbl supports OPS_READ only; use ops_arg_reduce" % where)
+        return LoopArg("gbl", unquote(inner[2]), inner[1], acc)
+    if fn == "ops_arg_reduce":
+        if len(inner) != 4:
+            raise SystemExit("%s: ops_arg_reduce needs 4 arguments: %s" % (where, text))
+        acc = inner[3].strip()
+        if acc not in ("OPS_INC", "OPS_MIN", "OPS_MAX"):
+            raise SystemExit("%s: ops_arg_reduce access must be INC/MIN/MAX" % where)
+        return LoopArg("reduce", unquote(inner[2]), inner[1], acc)
+    if fn == "ops_arg_idx":
+        return LoopArg("idx", "int", "3", "OPS_READ")
+    raise SystemExit("%s: unsupported argument kind %s" % (where, fn))
+
+
+def parse_params(ptext: str) -> List[KernelParam]:
+    masked = mask_comments_strings(ptext)
+    out = []
+    for p in split_top(ptext, masked):
+        if not p or p == "void":
+            continue
+        t = re.sub(r"\s+", " ", p.strip())
+        m = re.match(r"^(const\s+)?ACC\s*<\s*([\w\s:]+?)\s*>\s*&\s*(\w+)$", t)
+        if m:
+            out.append(KernelParam(p, m.group(2).strip(), True, bool(m.group(1)), m.group(3)))
+            continue
+        m = re.match(r"^(const\s+)?([\w\s:]+?)\s*(const\s*)?\*\s*(?:__restrict__\s*|restrict\s*)?(\w+)$", t)
+        if m:
+            out.append(KernelParam(p, m.group(2).strip(), False,
+                                   bool(m.group(1) or m.group(3)), m.group(4)))
+            continue
+        raise SystemExit("unsupported kernel parameter form: '%s'" % p)
+    return out
+
+
+FUNC_RE = re.compile(
+    r"((?:(?:static|inline|__forceinline__|__host__|__device__|OPS_FUN_PREFIX|constexpr)\s+)*)"
+    r"([\w:<>\s\*&]+?)\s*\b(\w+)\s*\(([^{};]*)\)\s*(?:const\s*)?$", re.S)
+
+
+def top_level_functions(text: str, header: str) -> List[KernelDef]:
+    """Top-level function definitions of a header (name, params, full text)."""
+    masked = mask_comments_strings(text)
+    # drop preprocessor lines from consideration (keep offsets)
+    lines = masked.split("\n")
+    pos = 0
+    masked_l = list(masked)
+    for ln in lines:
+        if ln.lstrip().startswith("#"):
+            for k in range(pos, pos + len(ln)):
+                masked_l[k] = " "
+        pos += len(ln) + 1
+    masked = "".join(masked_l)
+    res = []
+    depth = 0
+    i = 0
+    last_stmt_end = 0
+    n = len(masked)
+    while i < n:
+        ch = masked[i]
+        if ch == "{" and depth == 0:
+            head = masked[last_stmt_end:i]
+            close = match_paren(masked, i)
+            m = FUNC_RE.search(head.strip())
+            hs = head.strip()
+            if m and not re.match(r"^(struct|class|union|enum|namespace|extern)\b", hs) \
+                    and m.group(3) not in ("if", "for", "while", "switch"):
+                start = last_stmt_end + (len(head) - len(head.lstrip()))
+                full = text[start:close + 1]
+                seg = masked[last_stmt_end:i]
+                try:
+                    params = parse_params(seg[seg.index("(", seg.find(m.group(3))) + 1:
+                                              seg.rindex(")")])
+                except SystemExit:
+                    params = None
+                res.append((m.group(3), params, full))
+            i = close + 1
+            last_stmt_end = i
+            continue
+        if ch == ";" and depth == 0:
+            last_stmt_end = i + 1
+        i += 1
+    return [KernelDef(nm, prm, full, header) for nm, prm, full in res]
+
+
+# --------------------------------------------------------------------------
+# translator
+# --------------------------------------------------------------------------
+
+
+class Translator:
+    def __init__(self, sources: List[str], include_dirs: List[str], app: str, outdir: str):
+        self.sources = sources
+        self.include_dirs = include_dirs
+        self.app = app
+        self.outdir = outdir
+        self.loops: Dict[Tuple, Loop] = {}
+        self.call_sites: Dict[str, List[Tuple[int, int, str]]] = {}
+        self.consts: Dict[str, ConstDecl] = {}
+        self.kernels: Dict[str, KernelDef] = {}
+        self.helpers: Dict[str, KernelDef] = {}
+        self.headers: List[str] = []
+        self.header_includes: List[str] = []
+        self.ndim = 0
+
+    # -- discovery ---------------------------------------------------------
+    def resolve_include(self, name: str, from_dir: str) -> Optional[str]:
+        for d in [from_dir] + self.include_dirs:
+            p = os.path.join(d, name)
+            if os.path.isfile(p):
+                return os.path.abspath(p)
+        return None
+
+    def quoted_includes(self, path: str) -> List[str]:
+        try:
+            src = mask_comments_strings(open(path).read(), keep_strings=True)
+        except OSError:
+            return []
+        res = []
+        for m in re.finditer(r'^\s*#\s*include\s*"([^"]+)"', src, re.M):
+            inc = m.group(1)
+            if inc.startswith("ops_") or not inc.endswith(".h"):
+                continue
+            p = self.resolve_include(inc, os.path.dirname(path))
+            if p:
+                res.append(p)
+        return res
+
+    def scan_headers(self, path: str, seen: set) -> None:
+        for p in self.quoted_includes(path):
+            if p not in seen:
+                seen.add(p)
+                self.headers.append(p)
+                self.scan_headers(p, seen)
+
+    @staticmethod
+    def is_kernel_header(path: str) -> bool:
+        b = os.path.basename(path)
+        return b.endswith("kernel.h") or b.endswith("kernels.h")
+
+    def cu_includes(self) -> List[str]:
+        """Headers the device code needs: user_types.h (OPS convention for
+        types shared with kernels) and whatever the kernel headers include."""
+        out: List[str] = []
+        dirs = {os.path.dirname(s) for s in self.sources} | set(self.include_dirs)
+        for d in sorted(dirs):
+            p = os.path.join(d, "user_types.h")
+            if os.path.isfile(p) and os.path.abspath(p) not in out:
+                out.append(os.path.abspath(p))
+
+        def walk(h: str, seen: set) -> None:
+            for p in self.quoted_includes(h):
+                if p in seen or self.is_kernel_header(p):
+                    continue
+                seen.add(p)
+                walk(p, seen)
+                if p not in out:
+                    out.append(p)
+        seen: set = set()
+        for h in self.headers:
+            if self.is_kernel_header(h):
+                walk(h, seen)
+        return out
+
+    def run(self) -> None:
+        seen: set = set()
+        for s in self.sources:
+            self.scan_headers(s, seen)
+        for h in self.headers:
+            text = open(h).read()
+            for kd in top_level_functions(text, h):
+                if kd.params is not None and kd.name not in self.kernels:
+                    self.kernels[kd.name] = kd
+                self.helpers.setdefault(kd.name, kd)
+        for s in self.sources:
+            src = open(s).read()
+            m = re.search(r"#\s*define\s+OPS_(\d)D\b", src)
+            if m:
+                self.ndim = max(self.ndim, int(m.group(1)))
+            self.parse_source(s, src)
+        if self.ndim == 0:
+            self.ndim = max([l.ndim for l in self.loops.values()] + [2])
+        self.assign_stub_names()
+        os.makedirs(self.outdir, exist_ok=True)
+        for s in self.sources:
+            self.write_source(s)
+        self.write_kernels()
+
+    def parse_source(self, path: str, src: str) -> None:
+        where = os.path.basename(path)
+        sites = []
+        for start, end, args in find_calls(src, "ops_par_loop"):
+            if len(args) < 5:
+                raise SystemExit("%s: ops_par_loop with fewer than 5 arguments" % where)
+            kname = args[0].strip()
+            try:
+                ndim = int(args[3].strip())
+            except ValueError:
+                raise SystemExit("%s: ops_par_loop dim must be a literal: %s" % (where, args[3]))
+            largs = [parse_arg(a, where) for a in args[5:]]
+            loop = Loop(kname, ndim, largs)
+            k = loop.key()
+            if k not in self.loops:
+                self.loops[k] = loop
+            self.loops[k].sources.append(where)
+            sites.append((start, end, k, args))
+        self.call_sites[path] = sites
+        for fn in ("ops_decl_const", "ops_decl_const2", "ops_update_const"):
+            for _, _, args in find_calls(src, fn):
+                if len(args) != 4:
+                    continue
+                name = unquote(args[0])
+                ctype = unquote(args[2]).split(":")[0].strip()
+                if name not in self.consts:
+                    self.consts[name] = ConstDecl(name, args[1].strip(), ctype)
+
+    def assign_stub_names(self) -> None:
+        used: Dict[str, int] = {}
+        for k, loop in self.loops.items():
+            n = used.get(loop.kernel, 0)
+            used[loop.kernel] = n + 1
+            loop.stub = "ops_par_loop_%s" % loop.kernel + ("" if n == 0 else "_v%d" % n)
+
+    # -- source rewrite ------------------------------------------------------
+    def stub_proto(self, loop: Loop) -> str:
+        args = ", ".join("ops_arg" for _ in loop.args)
+        return "void %s(char const *, ops_block, int, int *%s);" % (
+            loop.stub, (", " + args) if args else "")
+
+    def write_source(self, path: str) -> None:
+        src = open(path).read()
+        sites = self.call_sites.get(path, [])
+        out = []
+        last = 0
+        for start, end, k, args in sites:
+            loop = self.loops[k]
+            out.append(src[last:start])
+            out.append("%s(%s)" % (loop.stub, ", ".join(args[1:])))
+            last = end
+        out.append(src[last:])
+        body = "".join(out)
+        protos = "\n".join(self.stub_proto(l) for l in self.loops.values())
+        hdr = ('#include "ops_lib_core.h"\n#include "ops_tridiag.h"\n'
+               "/* generated par_loop stubs (B200 backend) */\n%s\n" % protos)
+        body, nsub = re.subn(r'^\s*#\s*include\s*[<"]ops_seq(_v2)?\.h[>"].*$', hdr.rstrip("\n"),
+                             body, count=1, flags=re.M)
+        if nsub == 0:
+            body = hdr + body
+        base = os.path.splitext(os.path.basename(path))[0]
+        with open(os.path.join(self.outdir, base + "_ops.cpp"), "w") as f:
+            f.write("/* generated from %s by the OPS B200 translator */\n" % os.path.basename(path))
+            f.write('#line 1 "%s"\n' % os.path.abspath(path))
+            f.write(body)
+
+    # -- kernels file --------------------------------------------------------
+    def const_decl(self, c: ConstDecl) -> str:
+        d = c.dim.strip()
+        if d == "1":
+            return "__constant__ %s %s;" % (c.ctype, c.name)
+        if re.fullmatch(r"\d+", d):
+            return "__constant__ %s %s[%s];" % (c.ctype, c.name, d)
+        # run-time length: fixed-capacity symbol, checked at copy time
+        return "__constant__ %s %s[OB2_CONST_CAP(%s)];" % (c.ctype, c.name, c.ctype)
+
+    def write_kernels(self) -> None:
+        L: List[str] = []
+        w = L.append
+        w("/* generated by the OPS B200 translator: kernels of application '%s' */" % self.app)
+        w("#define OPS_%dD" % self.ndim)
+        w("#ifndef OPS_FUN_PREFIX")
+        w("#define OPS_FUN_PREFIX __host__ __device__")
+        w("#endif")
+        w('#include "ops_lib_core.h"')
+        w('#include "ops_b200_loop.h"')
+        w('#include "ops_b200_kernel.h"')
+        w("#include <cuda_runtime.h>")
+        # user headers that kernel headers depend on (types, macros)
+        for h in self.cu_includes():
+            w('#include "%s"' % h)
+        w("#define OB2_CONST_CAP(T) ((4096 + sizeof(T) - 1) / sizeof(T))")
+        w("namespace ob2_%s {" % re.sub(r"\W", "_", self.app))
+        for c in self.consts.values():
+            w(self.const_decl(c))
+        # all functions of the kernel headers, as device functions
+        emitted = set()
+        for h in self.headers:
+            if not self.is_kernel_header(h):
+                continue
+            for kd in top_level_functions(open(h).read(), h):
+                if kd.name in emitted:
+                    continue
+                emitted.add(kd.name)
+                text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
+                w("static __device__ __forceinline__ " + text)
+        for loop in self.loops.values():
+            if loop.kernel not in self.kernels:
+                raise SystemExit("kernel %s not found in the included headers" % loop.kernel)
+            if loop.kernel not in emitted:
+                kd = self.kernels[loop.kernel]
+                text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
+                w("static __device__ __forceinline__ " + text)
+                emitted.add(loop.kernel)
+        for loop in self.loops.values():
+            self.emit_loop(loop, w)
+        # constant copier
+        w("static int ob2_const_copy(const char *name, int dim, int type_size, const char *data,"
+          " void *stream) {")
+        for c in self.consts.values():
+            w('  if (!strcmp(name, "%s")) {' % c.name)
+            w("    size_t cap = sizeof(%s);" % c.name)
+            w("    size_t n = (size_t)dim * (size_t)type_size;")
+            w("    if (n > cap) return -1;")
+            w("    return (int)cudaMemcpyToSymbolAsync(%s, data, n, 0, cudaMemcpyHostToDevice,"
+              " (cudaStream_t)stream);" % c.name)
+            w("  }")
+        w("  return 0;")
+        w("}")
+        w("struct ob2_const_registrar { ob2_const_registrar() {"
+          " ob2_register_const_handler(&ob2_const_copy); } };")
+        w("static ob2_const_registrar ob2_const_registrar_instance;")
+        w("}  // namespace")
+        with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
+            f.write("\n".join(L) + "\n")
+
+    def emit_loop(self, loop: Loop, w) -> None:
+        kd = self.kernels[loop.kernel]
+        if len(kd.params) != len(loop.args):
+            raise SystemExit("kernel %s takes %d parameters but the loop passes %d arguments" %
+                             (loop.kernel, len(kd.params), len(loop.args)))
+        nd = loop.ndim
+        P = "ob2p_" + loop.stub[len("ops_par_loop_"):]
+        K = "ob2k_" + loop.stub[len("ops_par_loop_"):]
+        w("struct %s {" % P)
+        w("  int lo0, lo1, lo2, hi0, hi1, hi2;")
+        w("  unsigned int *counter;")
+        reds = []
+        for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+            if a.kind == "dat":
+                if not p.is_acc:
+                    raise SystemExit("kernel %s parameter %d must be an ACC<> for ops_arg_dat" %
+                                     (loop.kernel, i))
+                w("  %s *b%d; long long wx%d, wy%d, wz%d; int ex%d, ey%d, ez%d, ed%d;" %
+                  (p.base_type, i, i, i, i, i, i, i, i))
+            elif a.kind == "gbl":
+                w("  %s g%d[%s];" % (p.base_type, i, a.dim))
+            elif a.kind == "reduce":
+                w("  %s *r%d; %s *part%d; int first%d;" % (p.base_type, i, p.base_type, i, i))
+                reds.append((i, a, p))
+        w("};")
+        w("__global__ void __launch_bounds__(512) %s(const __grid_constant__ %s p) {" % (K, P))
+        w("  const int x = p.lo0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);")
+        w("  const int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);")
+        w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
+        for i, a, p in reds:
+            w("  %s red%d[%s];" % (p.base_type, i, a.dim))
+            w("  for (int d = 0; d < (%s); d++) red%d[d] = ob2::identity<%s, %s>();" %
+              (a.dim, i, p.base_type, a.acc))
+        w("  if (x < p.hi0 && y < p.hi1 && z < p.hi2) {")
+        call = []
+        for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+            if a.kind == "dat":
+                ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
+                w("    ACC<%s> a%d(p.b%d ? p.b%d + x * p.wx%d + y * p.wy%d + z * p.wz%d : "
+                  "(%s *)0, %s, p.ey%d, p.ez%d, p.ed%d);" %
+                  (p.base_type, i, i, i, i, i, i, p.base_type, ex, i, i, i))
+                call.append("a%d" % i)
+            elif a.kind == "gbl":
+                call.append("(%s *)p.g%d" % (p.base_type, i))
+            elif a.kind == "reduce":
+                call.append("red%d" % i)
+            elif a.kind == "idx":
+                call.append("idx")
+        if any(a.kind == "idx" for a in loop.args):
+            w("    int idx[3] = {x, y, z};")
+        w("    %s(%s);" % (loop.kernel, ", ".join(call)))
+        w("  }")
+        if reds:
+            w("  __shared__ double ob2_sh_raw[32 * 2];")
+            w("  __shared__ int ob2_flag;")
+            for i, a, p in reds:
+                w("  ob2::block_partial<%s, %s>(red%d, %s, p.part%d, (%s *)ob2_sh_raw);" %
+                  (p.base_type, a.acc, i, a.dim, i, p.base_type))
+            w("  if (ob2::last_block(p.counter, &ob2_flag)) {")
+            for i, a, p in reds:
+                w("    ob2::final_combine<%s, %s>(%s, p.part%d, p.r%d, p.first%d, (%s *)ob2_sh_raw);" %
+                  (p.base_type, a.acc, a.dim, i, i, i, p.base_type))
+            w("    ob2::reset_counter(p.counter);")
+            w("  }")
+        w("}")
+        # host stub
+        params = ", ".join("ops_arg arg%d" % i for i in range(len(loop.args)))
+        ns = re.sub(r"\W", "_", self.app)
+        w("}  // namespace")
+        w("void %s(char const *name, ops_block block, int dim, int *range%s) {" %
+          (loop.stub, (", " + params) if params else ""))
+        w("  using namespace ob2_%s;" % ns)
+        na = len(loop.args)
+        w("  ops_arg args[%d] = {%s};" % (max(na, 1), ", ".join("arg%d" % i for i in range(na))
+                                          or "ops_arg_idx()"))
+        w("  ob2_loop L;")
+        w("  if (!ob2_loop_begin(&L, name, block, dim, range, args, %d)) return;" % na)
+        w("  %s p;" % P)
+        w("  p.lo0 = L.lo[0]; p.lo1 = L.lo[1]; p.lo2 = L.lo[2];")
+        w("  p.hi0 = L.hi[0]; p.hi1 = L.hi[1]; p.hi2 = L.hi[2];")
+        w("  p.counter = L.counter;")
+        w("  dim3 blk(L.block[0], L.block[1], L.block[2]);")
+        w("  dim3 grd((L.n[0] + blk.x - 1) / blk.x, (L.n[1] + blk.y - 1) / blk.y,"
+          " (L.n[2] + blk.z - 1) / blk.z);")
+        if reds:
+            w("  size_t nblk = (size_t)grd.x * grd.y * grd.z;")
+            w("  char *scratch = (char *)L.partials;")
+        for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+            if a.kind == "dat":
+                w("  p.b%d = (%s *)L.view[%d].base; p.wx%d = L.view[%d].wx; p.wy%d = L.view[%d].wy;"
+                  " p.wz%d = L.view[%d].wz;" % (i, p.base_type, i, i, i, i, i, i, i))
+                w("  p.ex%d = L.view[%d].ex; p.ey%d = L.view[%d].ey; p.ez%d = L.view[%d].ez;"
+                  " p.ed%d = L.view[%d].ed;" % (i, i, i, i, i, i, i, i))
+            elif a.kind == "gbl":
+                w("  if ((size_t)arg%d.dim * (size_t)arg%d.elem_size > sizeof(p.g%d))"
+                  " throw OPSException(OPS_INVALID_ARGUMENT, \"Error: ops_arg_gbl larger than"
+                  " declared in the par_loop\");" % (i, i, i))
+                w("  memcpy(p.g%d, arg%d.data, (size_t)arg%d.dim * (size_t)arg%d.elem_size);" %
+                  (i, i, i, i))
+            elif a.kind == "reduce":
+                w("  p.r%d = (%s *)L.red[%d].acc; p.first%d = L.red[%d].first;" %
+                  (i, p.base_type, i, i, i))
+                w("  p.part%d = (%s *)scratch;"
+                  " scratch += ((nblk * (%s) * sizeof(%s) + 255) / 256) * 256;" %
+                  (i, p.base_type, a.dim, p.base_type))
+        w("  %s<<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
+        w("  ob2_loop_check_launch(&L);")
+        w("  ob2_loop_end(&L);")
+        w("}")
+        w("namespace ob2_%s {" % ns)
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description="OPS -> B200 translator")
+    ap.add_argument("sources", nargs="+")
+    ap.add_argument("-I", dest="incs", action="append", default=[])
+    ap.add_argument("--app", default=None)
+    ap.add_argument("--out", default=".")
+    a = ap.parse_args(argv)
+    app = a.app or os.path.splitext(os.path.basename(a.sources[0]))[0]
+    Translator([os.path.abspath(s) for s in a.sources], a.incs, app, a.out).run()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
