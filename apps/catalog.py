@@ -1,0 +1,197 @@
+"""Catalogue of the OPS applications used by the tests and the benchmark, and
+how to build each one in every flavour.
+
+Flavours
+  b200     this backend: translator + libops_b200.so (sm_100a)
+  oracle   the CPU oracle: oracle/include/ops_seq_v2.h + liboracle_ops.so
+  ref_seq  the reference's own sequential backend (ops_seq_v2.h + libops_seq.a)
+  ref_omp  the reference's own OpenMP backend (legacy translator + libops_seq.a)
+
+Applications are either this repository's drivers under apps/ (our code, on the
+unchanged OPS API) or reference applications, whose sources are read from the
+reference tree at build time only.  Every build of a reference application,
+and every ref_* flavour, goes under oracle/_ref/ (git-ignored; the built
+binaries travel to the GPU machine, the sources do not).
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+REF = os.environ.get("OPS_REFERENCE_TREE", "/root/reference")
+ORACLE_LIB_DIR = os.path.join(ROOT, "oracle", "_build")
+REF_OUT = os.path.join(ROOT, "oracle", "_ref")
+
+CLOVER_SRCS = ["clover_leaf.cpp", "initialise_chunk.cpp", "generate.cpp", "ideal_gas.cpp",
+               "update_halo.cpp", "field_summary.cpp", "viscosity.cpp", "calc_dt.cpp", "PdV.cpp",
+               "revert.cpp", "accelerate.cpp", "flux_calc.cpp", "advec_cell.cpp",
+               "advec_mom.cpp", "reset_field.cpp", "start.cpp", "time_step.cpp",
+               "build_field.cpp", "read_input.cpp", "initialise.cpp", "advection.cpp"]
+
+# name -> (kind, source dir, sources, translated sources (legacy translator))
+APPS = {
+    "poisson_mb": ("own", os.path.join(ROOT, "apps", "poisson_mb"), ["poisson_mb.cpp"], None),
+    "adi3d": ("own", os.path.join(ROOT, "apps", "adi3d"), ["adi3d.cpp"], None),
+    "heat_cg": ("own", os.path.join(ROOT, "apps", "heat_cg"), ["heat_cg.cpp"], None),
+    "opsunit": ("own", os.path.join(ROOT, "apps", "opsunit"), ["opsunit.cpp"], None),
+    "ref_poisson": ("ref", os.path.join(REF, "apps", "c", "poisson"), ["poisson.cpp"], None),
+    "ref_mblock": ("ref", os.path.join(REF, "apps", "c", "mblock"), ["mblock.cpp"], None),
+    "ref_laplace": ("ref", os.path.join(REF, "apps", "c", "laplace2d_tutorial", "step7"),
+                    ["laplace2d.cpp"], None),
+    "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
+                   CLOVER_SRCS[:15]),
+    # the CloverLeaf step harness: the CloverLeaf sources plus apps/clover_step
+    "clover_step": ("mixed", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
+                    CLOVER_SRCS[:15]),
+}
+CLOVER_STEP_SRC = os.path.join(ROOT, "apps", "clover_step", "clover_step.cpp")
+
+
+def build_dir(name: str, flavour: str) -> str:
+    kind = APPS[name][0]
+    if kind == "own" and not flavour.startswith("ref_"):
+        return os.path.join(ROOT, "apps", name, "_build", flavour)
+    return os.path.join(REF_OUT, "apps", name, flavour)
+
+
+def artifact(name: str, flavour: str, shared: bool = False) -> str:
+    d = build_dir(name, flavour)
+    return os.path.join(d, ("lib%s.so" % name) if shared else name)
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout[-4000:] + r.stderr[-8000:])
+        raise RuntimeError("build step failed: %s" % " ".join(cmd[:3]))
+    return r
+
+
+def sources_of(name: str):
+    kind, d, srcs, _ = APPS[name]
+    paths = [os.path.join(d, s) for s in srcs]
+    if name == "clover_step":
+        paths.append(CLOVER_STEP_SRC)
+    return d, paths
+
+
+def available(name: str) -> bool:
+    d, paths = sources_of(name)
+    return all(os.path.isfile(p) for p in paths)
+
+
+def ensure_oracle_lib() -> str:
+    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    return os.path.join(ORACLE_LIB_DIR, "liboracle_ops.so")
+
+
+def ensure_ref_lib() -> str:
+    if not os.path.isdir(REF):
+        raise RuntimeError("reference tree not present")
+    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "lib", "-j8", "REF=" + REF])
+    return os.path.join(REF_OUT, "lib", "libops_seq.a")
+
+
+def build(name: str, flavour: str, shared: bool = False, force: bool = False) -> str:
+    """Build one application flavour; returns the executable / library path."""
+    out = build_dir(name, flavour)
+    target = artifact(name, flavour, shared)
+    if os.path.exists(target) and not force:
+        return target
+    d, paths = sources_of(name)
+    os.makedirs(out, exist_ok=True)
+    extra_defs = []
+    if name == "clover_step":
+        extra_defs = ["-Dmain=clover_leaf_main"]
+    if flavour == "b200":
+        from ops_b200.build_app import build as b200_build
+        defs = [x[2:] for x in extra_defs]
+        if name == "clover_step":
+            # only clover_leaf.cpp's main is renamed; the harness keeps its own
+            return _build_b200_clover_step(out, d, paths, shared)
+        return b200_build(name, out, paths, [d], defines=defs, shared=shared)
+    if flavour == "oracle":
+        lib = ensure_oracle_lib()
+        inc = ["-I" + os.path.join(ROOT, "oracle", "include"), "-I" + os.path.join(ROOT, "include"),
+               "-I" + d]
+        objs = []
+        for p in paths:
+            o = os.path.join(out, os.path.basename(p) + ".o")
+            cmd = ["g++", "-O2", "-g", "-std=c++17", "-fPIC", "-w", *inc]
+            if name == "clover_step" and os.path.basename(p) == "clover_leaf.cpp":
+                cmd += extra_defs
+            if shared and name != "clover_step":
+                cmd += ["-Dmain=ops_app_main"]
+            _run(cmd + ["-c", p, "-o", o])
+            objs.append(o)
+        link = ["g++", "-o", target, *objs, "-L" + ORACLE_LIB_DIR, "-loracle_ops",
+                "-Wl,-rpath," + ORACLE_LIB_DIR]
+        if shared:
+            link[1:1] = ["-shared", "-Wl,-Bsymbolic"]
+        _run(link)
+        return target
+    if flavour in ("ref_seq", "ref_omp"):
+        lib = ensure_ref_lib()
+        rinc = os.path.join(REF, "ops", "c", "include")
+        srcdir = os.path.join(out, "src")
+        if os.path.isdir(srcdir):
+            shutil.rmtree(srcdir)
+        os.makedirs(srcdir)
+        for f in os.listdir(d):
+            if f.endswith((".cpp", ".h", ".in")):
+                shutil.copy(os.path.join(d, f), srcdir)
+        objs_src = [os.path.join(srcdir, os.path.basename(p)) for p in paths
+                    if p != CLOVER_STEP_SRC]
+        flags = ["-O3", "-std=c++14", "-fPIC", "-w", "-fopenmp", "-Dgnu", "-I" + rinc, "-I" + srcdir]
+        if flavour == "ref_omp":
+            trans = APPS[name][3] or APPS[name][2]
+            _run([sys.executable, os.path.join(REF, "ops_translator_legacy", "c", "ops.py"),
+                  *trans], cwd=srcdir)
+            objs_src = [os.path.join(srcdir, (s[:-4] + "_ops.cpp") if s in trans else s)
+                        for s in APPS[name][2]]
+            objs_src.append(os.path.join(srcdir, "mpi_openmp", "mpi_openmp_kernels.cpp"))
+        if name == "clover_step":
+            objs_src.append(CLOVER_STEP_SRC)
+        objs = []
+        for p in objs_src:
+            o = os.path.join(out, os.path.basename(p) + ".o")
+            cmd = ["g++", *flags]
+            if name == "clover_step" and os.path.basename(p).startswith("clover_leaf"):
+                cmd += extra_defs
+            if name == "clover_step" and p == CLOVER_STEP_SRC:
+                cmd += ["-DCLOVER_STEP_REFERENCE"]
+            _run(cmd + ["-c", p, "-o", o])
+            objs.append(o)
+        link = ["g++", "-fopenmp", "-o", target, *objs, lib]
+        if shared:
+            link[1:1] = ["-shared", "-Wl,-Bsymbolic"]
+        _run(link)
+        return target
+    raise ValueError(flavour)
+
+
+def _build_b200_clover_step(out, d, paths, shared):
+    from ops_b200.build_app import build as b200_build
+    return b200_build("clover_step", out, paths, [d], defines=[], shared=shared,
+                      rename_main={"clover_leaf.cpp": "clover_leaf_main"})
+
+
+def main(argv=None):
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("name")
+    ap.add_argument("flavour")
+    ap.add_argument("--shared", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(a.name, a.flavour, a.shared, a.force))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+/*
+ * Step-by-step driver for the CloverLeaf 2D application (an OPS user app,
+ * built unchanged from its own sources with clover_leaf.cpp's main renamed).
+ *
+ * The benchmark needs to time individual hydro steps with warm-up steps
+ * excluded, so this harness exposes the app's setup and one hydro step as C
+ * entry points.  setup mirrors the start of clover_leaf.cpp's main (ops_init,
+ * initialise, the ops_decl_const list, start) and a step is the body of its
+ * hydro loop (clover_leaf.cpp:180-199): timestep, PdV predict, accelerate,
+ * PdV correct, flux_calc, advection, reset_field, direction switch.
+ *
+ * The same file builds against this backend and against the reference
+ * OpenMP backend, so both are driven through identical calls.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#define OPS_2D
+#include "ops_seq_v2.h"
+#include "data.h"
+#include "definitions.h"
+
+void initialise();
+void field_summary();
+void timestep();
+void PdV(int predict);
+void accelerate();
+void flux_calc();
+void advection(int);
+void reset_field();
+void start();
+
+extern double g_small, g_big, dtc_safe, dtu_safe, dtv_safe, dtdiv_safe, dt, clover_time;
+extern double end_time;
+extern int number_of_states, g_circ, g_point, g_rect, step, advect_x, complete, end_step;
+extern FILE *g_out;
+
+extern "C" {
+
+/* Reads clover.in from the current directory. */
+__attribute__((visibility("default"))) int clover_step_setup(int argc, char **argv) {
+  ops_init(argc, argv, 1);
+  initialise();
+  ops_decl_const("g_small", 1, "double", &g_small);
+  ops_decl_const("g_big", 1, "double", &g_big);
+  ops_decl_const("dtc_safe", 1, "double", &dtc_safe);
+  ops_decl_const("dtu_safe", 1, "double", &dtu_safe);
+  ops_decl_const("dtv_safe", 1, "double", &dtv_safe);
+  ops_decl_const("dtdiv_safe", 1, "double", &dtdiv_safe);
+  ops_decl_const("field", 1, "field_type", &field);
+  ops_decl_const("grid", 1, "grid_type", &grid);
+  ops_decl_const("number_of_states", 1, "int", &number_of_states);
+  ops_decl_const("states", number_of_states, "state_type", states);
+  ops_decl_const("g_circ", 1, "int", &g_circ);
+  ops_decl_const("g_point", 1, "int", &g_point);
+  ops_decl_const("g_rect", 1, "int", &g_rect);
+  ops_decl_const("dt", 1, "double", &dt);
+  start();
+  return 0;
+}
+
+/* Runs n hydro steps; returns the simulated time reached. */
+__attribute__((visibility("default"))) double clover_step_run(int n) {
+  for (int i = 0; i < n; i++) {
+    step = step + 1;
+    timestep();
+    PdV(TRUE);
+    accelerate();
+    PdV(FALSE);
+    flux_calc();
+    advection(step);
+    reset_field();
+    advect_x = (advect_x == TRUE) ? FALSE : TRUE;
+    clover_time = clover_time + dt;
+  }
+  return clover_time;
+}
+
+/* field_summary of the app (writes the summary line to clover.out). */
+__attribute__((visibility("default"))) void clover_step_summary(void) {
+  complete = TRUE;
+  field_summary();
+  fflush(g_out);
+}
+
+__attribute__((visibility("default"))) int clover_step_current(void) { return step; }
+
+__attribute__((visibility("default"))) void clover_step_finish(void) {
+  fflush(g_out);
+  ops_exit();
+}
+
+}  // extern "C"

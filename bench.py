@@ -1,0 +1,387 @@
+"""Benchmark: OPS 2D compressible hydro (CloverLeaf application) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--cells 3840] [--no-baseline]
+
+Workload: the CloverLeaf 2D Lagrangian-Eulerian hydro application, unchanged
+OPS user code, on 3840 x 3840 cells (ideal gas gamma=1.4, background rho=0.2
+e=1.0, a seeded cell-aligned square of 1/16 of the domain at rho=1.0 e=2.5),
+FP64.  One step is one hydro time step of the application (~160 par_loops:
+timestep/calc_dt min reduction, ideal_gas, viscosity, PdV predictor and
+corrector, accelerate, flux_calc, advec_cell / advec_mom sweeps, reset_field
+and the 2-deep boundary halo loops).
+
+ours       the app built by the translator on libops_b200.so; steps timed
+           with CUDA events on the runtime's work stream; one process per GPU
+           under torchrun, each running its own replica (the path does not
+           shard across GPUs: replicas only, weak scaling).
+reference  the same app on the reference's own OpenMP backend (built from the
+           reference sources), all host cores, rank 0 only.
+
+Prints one JSON line (rank 0).  value = cell updates per second over all
+ranks (GLUPS).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GLUPS"
+UNIT = "GLUPS"
+WORKLOAD = "cloverleaf2d_hydro"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of kernels from a committed ncu summary
+    (profiles/ncu_traffic.txt: `kernel bytes_per_launch ...`)."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    except OSError:
+        pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# multi-process plumbing (torchrun): gloo on CPU tensors only; the GPU work is
+# entirely this backend's own, one replica per rank.
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def clover_lib(flavour: str) -> str:
+    from apps.catalog import artifact, available, build
+    lib = artifact("clover_step", flavour, shared=True)
+    if not os.path.exists(lib):
+        if not available("clover_step"):
+            raise FileNotFoundError("CloverLeaf %s build missing and its sources are not "
+                                    "present to build it" % flavour)
+        lib = build("clover_step", flavour, shared=True)
+    return lib
+
+
+def cpu_reference_run(cells, steps, warmup, threads, timeout=900):
+    """Reference OpenMP backend on the host cores, in its own process."""
+    cmd = [sys.executable, "-m", "apps.clover_run", "--flavour", "ref_omp", "--cells",
+           str(cells), "--steps", str(steps), "--warmup", str(warmup), "--threads",
+           str(threads)]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread",
+               OMP_PLACES="cores")
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=timeout, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+    return json.loads(line)
+
+
+def dominant_kernel(report: str):
+    rows = []
+    for line in report.splitlines():
+        p = line.rsplit(" ", 3)
+        if len(p) == 4:
+            rows.append((p[0], int(p[1]), float(p[2]), float(p[3])))
+    if not rows:
+        return None, rows
+    tot = sum(r[2] for r in rows)
+    top = max(rows, key=lambda r: r[2])
+    return (top, tot), rows
+
+
+def run_ours(a, d: Dist):
+    """Our arm on this rank's GPU: setup, W warm-up steps, K timed steps."""
+    import ctypes
+    os.environ["OPS_B200_DEVICE"] = str(d.local)
+    lib = clover_lib("b200")
+    from apps.clover_run import make_deck
+    work = tempfile.mkdtemp(prefix="clover_bench_")
+    with open(os.path.join(work, "clover.in"), "w") as f:
+        f.write(make_deck(a.cells, a.seed))
+    here = os.getcwd()
+    os.chdir(work)
+    L = ctypes.CDLL(lib, mode=ctypes.RTLD_GLOBAL)
+    B = ctypes.CDLL(os.path.join(ROOT, "ops_b200", "lib", "libops_b200.so"),
+                    mode=ctypes.RTLD_GLOBAL)
+    L.clover_step_run.restype = ctypes.c_double
+    B.ob2_launch_count.restype = ctypes.c_longlong
+    B.ob2_ktime_report.restype = ctypes.c_size_t
+    argv = (ctypes.c_char_p * 2)(b"clover_step", None)
+    L.clover_step_setup(1, argv)
+    L.clover_step_run(a.warmup)
+    B.ob2_dev_sync()
+    ev0, ev1 = ctypes.c_void_p(), ctypes.c_void_p()
+    B.ob2_event_create(ctypes.byref(ev0))
+    B.ob2_event_create(ctypes.byref(ev1))
+    B.ob2_ktime_reset()
+    B.ob2_ktime_enable(1 if a.ktime else 0)
+    n0 = B.ob2_launch_count()
+    clocks = ClockSampler(d.local)
+    d.barrier()
+    clocks.start()
+    B.ob2_event_record(ev0)
+    L.clover_step_run(a.steps)
+    B.ob2_event_record(ev1)
+    ms = ctypes.c_float()
+    rc = B.ob2_event_elapsed_ms(ev0, ev1, ctypes.byref(ms))
+    clk = clocks.stop()
+    if rc != 0:
+        raise RuntimeError("CUDA error %d in the timed region" % rc)
+    launches = B.ob2_launch_count() - n0
+    n = B.ob2_ktime_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    B.ob2_ktime_report(buf, n + 1)
+    report = buf.value.decode()
+    B.ob2_ktime_enable(0)
+    t_ms = d.max(ms.value)
+
+    # end to end through the C ABI: the hydro state (density0, energy0,
+    # xvel0, yvel0) comes in from pinned host buffers with ops_dat_set_data,
+    # K steps run, the same fields go back with ops_dat_fetch_data; host
+    # wall clock around all of it.
+    names = ["density0", "energy0", "xvel0", "yvel0"]
+    dats = [ctypes.c_void_p.in_dll(L, nm) for nm in names]
+    B.ops_dat_get_extents.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    bufs, nbytes = [], 0
+    for dd in dats:
+        sz = (ctypes.c_int * 2)()
+        B.ops_dat_get_extents(dd, 0, None, sz)
+        nb = sz[0] * sz[1] * 8
+        p = ctypes.c_void_p()
+        B.ob2_host_alloc_pinned(ctypes.byref(p), ctypes.c_size_t(nb))
+        B.ops_dat_fetch_data.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        B.ops_dat_fetch_data(dd, 0, p)
+        bufs.append(p)
+        nbytes += nb
+    B.ops_dat_set_data.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    B.ob2_dev_sync()
+    d.barrier()
+    t0 = time.perf_counter()
+    for dd, p in zip(dats, bufs):
+        B.ops_dat_set_data(dd, 0, p)
+    L.clover_step_run(a.steps)
+    for dd, p in zip(dats, bufs):
+        B.ops_dat_fetch_data(dd, 0, p)
+    e2e_s = d.max(time.perf_counter() - t0)
+    L.clover_step_summary()
+    L.clover_step_finish()
+    os.chdir(here)
+    return {"t_ms": t_ms, "launches": launches, "report": report, "clocks": clk,
+            "e2e_s": e2e_s, "e2e_state_bytes": nbytes}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=3840)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--no-ktime", dest="ktime", action="store_false")
+    ap.add_argument("--baseline-steps", type=int, default=2)
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        a.warmup = 3
+    cells_total = float(a.cells) * a.cells
+    config = {"workload": WORKLOAD, "cells": "%dx%d" % (a.cells, a.cells), "precision": "fp64",
+              "halo_depth": 2, "seed": a.seed,
+              "l2": "inputs larger than L2 (about 3 GB of FP64 fields per replica)"}
+
+    if a.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        cores = host_cores()
+        try:
+            r = cpu_reference_run(a.cells, a.steps, a.warmup, cores)
+        except Exception as e:  # noqa: BLE001
+            print(json.dumps({"impl": "reference", "unavailable": str(e).splitlines()[-1][:200]}))
+            return 0
+        v = cells_total / r["s_per_step"] / 1e9
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": r["s_per_step"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded input deck)", "impl": "reference",
+                "config": dict(config, parallelism="openmp %d threads" % cores),
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                 "sample": "%d steps after %d warm-up steps of the full config"
+                                           % (a.steps, a.warmup)},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    d = Dist()
+    res = run_ours(a, d)
+    value = cells_total * a.steps * d.world / (res["t_ms"] * 1e-3) / 1e9
+    launches = int(d.sum(res["launches"]))
+    e2e_v = cells_total * a.steps * d.world / res["e2e_s"] / 1e9
+    if d.rank == 0:
+        peak, peak_kind = measured_hbm()
+        dk, rows = dominant_kernel(res["report"])
+        roof = None
+        if dk:
+            (name, cnt, dms, byts), tot = dk
+            avg_s = dms * 1e-3 / cnt
+            achieved = (byts / cnt) / avg_s / 1e9
+            traffic = ncu_traffic().get(name)
+            roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": traffic, "algorithmic_bytes_per_launch": byts / cnt,
+                    "avg_launch_us": avg_s * 1e6, "share_of_device_time": dms / tot if tot else None}
+            step_bytes = sum(r[3] for r in rows) / a.steps
+            roof["step_algorithmic_GBps"] = step_bytes / (res["t_ms"] * 1e-3 / a.steps) / 1e9
+            roof["step_frac"] = roof["step_algorithmic_GBps"] / peak
+        base = None
+        if not a.no_baseline and d.world == 1:
+            cores = host_cores()
+            try:
+                r = cpu_reference_run(a.cells, a.baseline_steps, 1, cores)
+                base = {"value": cells_total / r["s_per_step"] / 1e9, "unit": UNIT,
+                        "cores": cores, "kind": "reference",
+                        "sample": "%d steps (after 1 warm-up) of the %dx%d config on the "
+                                  "reference OpenMP backend" % (a.baseline_steps, a.cells, a.cells)}
+            except Exception as e:  # noqa: BLE001
+                base = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                        "sample": "unavailable: " + str(e).splitlines()[-1][:160]}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": res["t_ms"] / a.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded input deck)",
+                "config": dict(config, parallelism="replicas x%d" % d.world),
+                "roofline": roof, "cpu_baseline": base,
+                "e2e": {"value": e2e_v, "unit": UNIT,
+                        "h2d_bytes_per_step": res["e2e_state_bytes"] / a.steps,
+                        "d2h_bytes_per_step": res["e2e_state_bytes"] / a.steps,
+                        "note": "state in from and out to pinned host buffers around K steps"},
+                "gpu_launches": launches, "clocks": res["clocks"]}
+        print(json.dumps(line), flush=True)
+    d.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

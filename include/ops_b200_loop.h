@@ -61,6 +61,18 @@ OPS_API void ob2_loop_end(ob2_loop *L);
 /* Checks the launch just issued; throws OPSException on error. */
 OPS_API void ob2_loop_check_launch(ob2_loop *L);
 
+/* Per-kernel device timing.  While enabled, every launch (par_loops, halo
+ * transfers, tridiagonal solves) is bracketed by CUDA events on the work
+ * stream without any host synchronisation.  ob2_ktime_report resolves them
+ * and writes one line per kernel: "name launches device_ms algorithmic_bytes"
+ * (bytes by the OPS transfer model, ops_lib_core.cpp:1687-1697), returning
+ * the full length.  ob2_ktime_reset clears the counters of every kernel. */
+OPS_API void ob2_ktime_enable(int on);
+OPS_API void ob2_ktime_reset(void);
+OPS_API size_t ob2_ktime_report(char *buf, size_t n);
+/* Kernels launched by the runtime since ops_init. */
+OPS_API long long ob2_launch_count(void);
+
 /* Constant registry: the generated kernels file registers one callback that
  * copies a named constant into its __constant__ symbol. */
 typedef int (*ob2_const_fn)(const char *name, int dim, int type_size, const char *data,

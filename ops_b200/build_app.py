@@ -51,7 +51,9 @@ def ensure_lib(verbose=False):
 
 
 def build(app, out, sources, incs, defines=(), shared=False, verbose=False, jobs=8,
-          extra_nvcc=()):
+          extra_nvcc=(), rename_main=None):
+    """rename_main: {source basename: new name} renames that source's main
+    (used by harnesses that drive an app's functions themselves)."""
     ensure_lib(verbose)
     os.makedirs(out, exist_ok=True)
     gen = os.path.join(out, "gen")
@@ -75,7 +77,9 @@ def build(app, out, sources, incs, defines=(), shared=False, verbose=False, jobs
         o = os.path.join(out, base + "_ops.o")
         cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-w", *common,
                "-I" + os.path.join(CUDA, "include"), "-c", g, "-o", o]
-        if shared:
+        if rename_main and os.path.basename(s) in rename_main:
+            cmd.insert(1, "-Dmain=" + rename_main[os.path.basename(s)])
+        elif shared and not rename_main:
             cmd.insert(1, "-Dmain=ops_app_main")
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
                                        text=True), g))
@@ -94,7 +98,9 @@ def build(app, out, sources, incs, defines=(), shared=False, verbose=False, jobs
     link = [NVCC, *ARCH, "-o", target, *objs, "-L" + LIBDIR, "-lops_b200",
             "-Xlinker", "-rpath=" + LIBDIR, "-L" + os.path.join(CUDA, "lib64"), "-lcudart"]
     if shared:
-        link.insert(1, "-shared")
+        # -Bsymbolic: the app's own globals must bind inside the library
+        # (glibc exports names such as `step` that would interpose them)
+        link[1:1] = ["-shared", "-Xlinker", "-Bsymbolic"]
     run(link, verbose)
     return target
 

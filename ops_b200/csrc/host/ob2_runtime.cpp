@@ -80,7 +80,13 @@ struct Runtime {
   size_t stage_cap = 0;
   unsigned long long rng_seed = 0, rng_counter = 0;
   ob2_const_fn const_fn = nullptr;
-  ob2_loop *loop_events = nullptr;
+  // per-kernel device timing without host synchronisation: event pairs are
+  // recorded around every launch and resolved by ob2_ktime_collect()
+  bool ktime = false;
+  std::vector<void *> ev_pool;
+  struct Pending { void *a, *b; int k; };
+  std::vector<Pending> pending;
+  long long launches = 0;  // kernels launched by this runtime
 };
 
 Runtime *R = nullptr;
@@ -221,6 +227,34 @@ int kernel_slot(const char *name) {
   r.kstats.back().name = name;
   r.kindex[name] = k;
   return k;
+}
+
+void *pool_event() {
+  Runtime &r = rt();
+  void *e = nullptr;
+  if (!r.ev_pool.empty()) {
+    e = r.ev_pool.back();
+    r.ev_pool.pop_back();
+  } else {
+    check(ob2_event_create(&e), "event");
+  }
+  return e;
+}
+
+/* start / end of one timed launch of kernel slot k (ktime mode) */
+void *kt_begin() {
+  if (!rt().ktime) return nullptr;
+  void *a = pool_event();
+  ob2_event_record(a);
+  return a;
+}
+void kt_end(void *a, int k) {
+  Runtime &r = rt();
+  r.launches++;
+  if (!a) return;
+  void *b = pool_event();
+  ob2_event_record(b);
+  r.pending.push_back({a, b, k});
 }
 
 }  // namespace
@@ -664,8 +698,10 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
   }
   int k = kernel_slot("ops_halo_transfer");
   double t0 = wall();
+  void *ev = kt_begin();
   check(ob2_halo_run((const ob2_halo_task *)gx.tasks_d, gx.ntasks, gx.max_pts),
         "ops_halo_transfer");
+  kt_end(ev, k);
   KStat &s = rt().kstats[k];
   s.count++;
   s.host_s += wall() - t0;
@@ -826,7 +862,9 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->partials = r.partials;
   L->partials_bytes = r.partials_cap;
   L->counter = r.counter;
-  if (r.inst.OPS_diags > 1) {
+  if (r.ktime) {
+    L->ev_start = kt_begin();
+  } else if (r.inst.OPS_diags > 1) {
     ob2_event_create(&L->ev_start);
     ob2_event_create(&L->ev_end);
     ob2_event_record(L->ev_start);
@@ -847,7 +885,11 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
   Runtime &r = rt();
   KStat &s = r.kstats[L->kernel_index];
   s.count++;
-  if (L->ev_start) {
+  if (r.ktime) {
+    kt_end(L->ev_start, L->kernel_index);
+    L->ev_start = nullptr;
+  } else if (L->ev_start) {
+    r.launches++;
     ob2_event_record(L->ev_end);
     float ms = 0.f;
     check(ob2_event_elapsed_ms(L->ev_start, L->ev_end, &ms), L->name);
@@ -855,6 +897,8 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
     ob2_event_destroy(L->ev_start);
     ob2_event_destroy(L->ev_end);
     L->ev_start = L->ev_end = nullptr;
+  } else {
+    r.launches++;
   }
   s.host_s += wall() - L->host_t0;
   for (int i = 0; i < L->nargs; i++) {
@@ -869,6 +913,54 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
                   ((a.acc == OPS_RW || a.acc == OPS_INC) ? 2.0 : 1.0);
   }
 }
+
+/* ------------------------------------------------------------------------
+ * per-kernel device timing (see ops_b200_loop.h)
+ * ---------------------------------------------------------------------- */
+static void ktime_collect() {
+  Runtime &r = rt();
+  if (r.pending.empty()) return;
+  check(ob2_dev_sync(), "ob2_ktime");
+  for (auto &p : r.pending) {
+    float ms = 0.f;
+    check(ob2_event_elapsed_ms(p.a, p.b, &ms), "ob2_ktime");
+    r.kstats[p.k].dev_ms += ms;
+    r.ev_pool.push_back(p.a);
+    r.ev_pool.push_back(p.b);
+  }
+  r.pending.clear();
+}
+OPS_API void ob2_ktime_enable(int on) {
+  ktime_collect();
+  rt().ktime = on != 0;
+}
+OPS_API void ob2_ktime_reset(void) {
+  ktime_collect();
+  for (auto &k : rt().kstats) {
+    k.count = 0;
+    k.dev_ms = 0.0;
+    k.host_s = 0.0;
+    k.transfer = 0.0;
+  }
+}
+OPS_API size_t ob2_ktime_report(char *buf, size_t n) {
+  ktime_collect();
+  std::string s;
+  char line[512];
+  for (auto &k : rt().kstats) {
+    if (!k.count) continue;
+    snprintf(line, sizeof line, "%s %ld %.6f %.0f\n", k.name.c_str(), k.count, k.dev_ms,
+             k.transfer);
+    s += line;
+  }
+  if (buf && n) {
+    size_t m = std::min(n - 1, s.size());
+    memcpy(buf, s.data(), m);
+    buf[m] = 0;
+  }
+  return s.size();
+}
+OPS_API long long ob2_launch_count(void) { return rt().launches; }
 
 /* ------------------------------------------------------------------------
  * output / timing (ops_lib_core.cpp:1468-1647)
@@ -1191,9 +1283,11 @@ static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_d
   size_t ts = a->type_size;
   int k = kernel_slot(u ? "ops_tridMultiDimBatch_Inc" : "ops_tridMultiDimBatch");
   double t0 = wall();
+  void *ev = kt_begin();
   int rc = ob2_trid_batch((int)ts, ndim, solvedim, dims, strides, a->data_d + off * ts,
                           b->data_d + off * ts, c->data_d + off * ts, d->data_d + off * ts,
                           u ? u->data_d + off * ts : nullptr);
+  kt_end(ev, k);
   if (rc) {
     OPSException ex(OPS_RUNTIME_ERROR);
     ex << "Tridsolver error: " << ob2_error_string(rc) << " (line length "
