@@ -98,11 +98,39 @@ def ensure_ref_lib() -> str:
     return os.path.join(REF_OUT, "lib", "libops_seq.a")
 
 
+def _deps(name: str, flavour: str):
+    d, paths = sources_of(name)
+    deps = list(paths)
+    for dd in {d, os.path.dirname(CLOVER_STEP_SRC) if name == "clover_step" else d}:
+        if os.path.isdir(dd):
+            deps += [os.path.join(dd, f) for f in os.listdir(dd) if f.endswith(".h")]
+    if flavour == "b200":
+        deps.append(os.path.join(ROOT, "ops_b200", "translator", "ops_translate.py"))
+        deps.append(os.path.join(ROOT, "ops_b200", "build_app.py"))
+        inc = os.path.join(ROOT, "include")
+        deps += [os.path.join(inc, f) for f in os.listdir(inc)]
+    elif flavour == "oracle":
+        deps += [os.path.join(ROOT, "oracle", "include", "ops_seq_v2.h"),
+                 os.path.join(ROOT, "include", "ops_lib_core.h")]
+    return [p for p in deps if os.path.exists(p)]
+
+
+def stale(name: str, flavour: str, shared: bool = False) -> bool:
+    target = artifact(name, flavour, shared)
+    if not os.path.exists(target):
+        return True
+    if not available(name):
+        return False  # prebuilt and no sources to rebuild from
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(p) > t for p in _deps(name, flavour))
+
+
 def build(name: str, flavour: str, shared: bool = False, force: bool = False) -> str:
-    """Build one application flavour; returns the executable / library path."""
+    """Build one application flavour (when missing or older than its
+    sources, headers or the translator); returns the executable / library."""
     out = build_dir(name, flavour)
     target = artifact(name, flavour, shared)
-    if os.path.exists(target) and not force:
+    if not force and not stale(name, flavour, shared):
         return target
     d, paths = sources_of(name)
     os.makedirs(out, exist_ok=True)

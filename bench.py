@@ -302,6 +302,8 @@ def main(argv=None):
     ap.add_argument("--no-baseline", action="store_true")
     ap.add_argument("--no-ktime", dest="ktime", action="store_false")
     ap.add_argument("--baseline-steps", type=int, default=2)
+    ap.add_argument("--report", action="store_true",
+                    help="print the per-kernel device-time table to stderr")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3
@@ -335,7 +337,17 @@ def main(argv=None):
         return 0
 
     d = Dist()
-    res = run_ours(a, d)
+    # the application prints progress on stdout: send the process's stdout to
+    # stderr while it runs so that stdout carries only the result line
+    sys.stdout.flush()
+    saved_stdout = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        res = run_ours(a, d)
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved_stdout, 1)
+        os.close(saved_stdout)
     value = cells_total * a.steps * d.world / (res["t_ms"] * 1e-3) / 1e9
     launches = int(d.sum(res["launches"]))
     e2e_v = cells_total * a.steps * d.world / res["e2e_s"] / 1e9
@@ -343,7 +355,9 @@ def main(argv=None):
         peak, peak_kind = measured_hbm()
         dk, rows = dominant_kernel(res["report"])
         roof = None
-        if dk:
+        if a.report:
+            sys.stderr.write("kernel launches device_ms algorithmic_bytes\n" + res["report"])
+        if dk and dk[0][2] > 0:
             (name, cnt, dms, byts), tot = dk
             avg_s = dms * 1e-3 / cnt
             achieved = (byts / cnt) / avg_s / 1e9

@@ -23,6 +23,7 @@
 /* ---- device / stream / memory (ops_cuda_common.cu:68-182) ---- */
 OB2_API int ob2_dev_init(int device);           /* cutilDeviceInit */
 OB2_API int ob2_dev_count(int *n);
+OB2_API int ob2_dev_sm_count(int *n);           /* SMs of the current device */
 OB2_API void *ob2_dev_stream(void);             /* the runtime's work stream */
 OB2_API int ob2_dev_set_stream(void *stream);   /* 0 restores the default work stream */
 OB2_API int ob2_dev_malloc(void **p, size_t n); /* ops_device_malloc */

@@ -51,6 +51,9 @@ typedef struct ob2_loop {
   void *ev_start, *ev_end;  /* timing events (diagnostics level > 1) */
   double host_t0;
   int block[3];             /* suggested CTA shape */
+  int grid[3];              /* suggested grid: x covers the range, y/z capped
+                               at about one full wave of resident CTAs; the
+                               kernel loops over the remaining y/z */
 } ob2_loop;
 
 /* Returns 0 when the range is empty (nothing to launch, ob2_loop_end not
@@ -58,6 +61,10 @@ typedef struct ob2_loop {
 OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int dim,
                            const int *range, ops_arg *args, int nargs);
 OPS_API void ob2_loop_end(ob2_loop *L);
+/* 1 when some dat is passed more than once and written through one of the
+ * arguments: the loop's kernel must then not assume its dat pointers are
+ * unaliased. */
+OPS_API int ob2_args_alias(const ops_arg *args, int nargs);
 /* Checks the launch just issued; throws OPSException on error. */
 OPS_API void ob2_loop_check_launch(ob2_loop *L);
 

@@ -39,6 +39,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #endif
 
 #if !defined(__CUDACC__)
@@ -334,6 +335,12 @@ enum {
 #ifdef __cplusplus
 OPS_API bool ops_checkpointing_init(const char *filename, double interval, int options);
 #endif
+/* HDF5 output (ops_hdf5.h:130-166): this backend has no HDF5; the calls
+ * report that on stderr and write nothing. */
+OPS_API void ops_fetch_dat_hdf5_file(ops_dat dat, char const *file_name);
+OPS_API void ops_fetch_block_hdf5_file(ops_block block, char const *file_name);
+OPS_API void ops_fetch_stencil_hdf5_file(ops_stencil stencil, char const *file_name);
+OPS_API void ops_fetch_halo_hdf5_file(ops_halo halo, char const *file_name);
 /* checked allocators used by apps (ops_util.h:41-45): abort on failure */
 OPS_API void *xmalloc(size_t size);
 OPS_API void *xrealloc(void *ptr, size_t size);
@@ -481,6 +488,24 @@ template <class T> void ops_update_const(char const *name, int dim, char const *
  * serves AoS and SoA layouts and strided (multigrid / low-dim) dats.
  * ------------------------------------------------------------------------- */
 #ifdef __cplusplus
+#ifdef __CUDA_ARCH__
+/* atomic min / max by compare-and-swap (floating point has no native one) */
+template <typename T> __device__ __forceinline__ void ob2_atomic_minmax(T *a, T v, bool is_min) {
+  static_assert(sizeof(T) == 8 || sizeof(T) == 4, "8- or 4-byte types only");
+  typedef typename std::conditional<sizeof(T) == 8, unsigned long long, unsigned int>::type U;
+  U *ua = (U *)a;
+  U old = *ua, assumed;
+  do {
+    assumed = old;
+    T cur;
+    memcpy(&cur, &assumed, sizeof(T));
+    if (is_min ? !(v < cur) : !(v > cur)) return;
+    U nv;
+    memcpy(&nv, &v, sizeof(T));
+    old = atomicCAS(ua, assumed, nv);
+  } while (old != assumed);
+}
+#endif
 template <typename T> class ACC {
  public:
   T *p;      /* component 0 of the current point */
@@ -493,6 +518,55 @@ template <typename T> class ACC {
   __host__ __device__ __forceinline__ ACC(T *ptr, int sx_, int sy_, int sz_, int sd_)
       : p(ptr), sx(sx_), sy(sy_), sz(sz_), sd(sd_) {}
   __host__ __device__ __forceinline__ void next(long elems) { p += elems; }
+
+  /* accumulation into shared points (low-dim dats): atomic on the device */
+  __host__ __device__ __forceinline__ static void acc_inc(T *a, T v) {
+#ifdef __CUDA_ARCH__
+    atomicAdd(a, v);
+#else
+    *a += v;
+#endif
+  }
+  __host__ __device__ __forceinline__ static void acc_min(T *a, T v) {
+#ifdef __CUDA_ARCH__
+    ob2_atomic_minmax(a, v, true);
+#else
+    if (v < *a) *a = v;
+#endif
+  }
+  __host__ __device__ __forceinline__ static void acc_max(T *a, T v) {
+#ifdef __CUDA_ARCH__
+    ob2_atomic_minmax(a, v, false);
+#else
+    if (v > *a) *a = v;
+#endif
+  }
+
+#if defined(OPS_1D)
+  __host__ __device__ __forceinline__ void combine_inc(int x, T v) const { acc_inc(&p[x * sx], v); }
+  __host__ __device__ __forceinline__ void combine_min(int x, T v) const { acc_min(&p[x * sx], v); }
+  __host__ __device__ __forceinline__ void combine_max(int x, T v) const { acc_max(&p[x * sx], v); }
+#elif defined(OPS_3D)
+  __host__ __device__ __forceinline__ void combine_inc(int x, int y, int z, T v) const {
+    acc_inc(&p[x * sx + y * sy + z * sz], v);
+  }
+  __host__ __device__ __forceinline__ void combine_min(int x, int y, int z, T v) const {
+    acc_min(&p[x * sx + y * sy + z * sz], v);
+  }
+  __host__ __device__ __forceinline__ void combine_max(int x, int y, int z, T v) const {
+    acc_max(&p[x * sx + y * sy + z * sz], v);
+  }
+#else
+  __host__ __device__ __forceinline__ void combine_inc(int x, int y, T v) const {
+    acc_inc(&p[x * sx + y * sy], v);
+  }
+  __host__ __device__ __forceinline__ void combine_min(int x, int y, T v) const {
+    acc_min(&p[x * sx + y * sy], v);
+  }
+  __host__ __device__ __forceinline__ void combine_max(int x, int y, T v) const {
+    acc_max(&p[x * sx + y * sy], v);
+  }
+#endif
 
 #if defined(OPS_1D)
   __host__ __device__ __forceinline__ T &operator()(int x) const { return p[x * sx]; }

@@ -66,6 +66,11 @@ def build(app, out, sources, incs, defines=(), shared=False, verbose=False, jobs
     procs = []
     cu = os.path.join(gen, app + "_kernels.cu")
     cu_o = os.path.join(out, app + "_kernels.o")
+    # IEEE arithmetic by default (no FMA contraction), as the reference's
+    # IEEE build (makefiles/Makefile.cuda:55-56): the generated kernels then
+    # round exactly like the host code of the same user kernels.
+    if os.environ.get("OPS_B200_FMAD", "0") != "1":
+        extra_nvcc = ("--fmad=false",) + tuple(extra_nvcc)
     procs.append((subprocess.Popen(
         [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-w", *extra_nvcc, *common, "-c", cu, "-o", cu_o],

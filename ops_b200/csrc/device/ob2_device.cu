@@ -38,6 +38,10 @@ OB2_API int ob2_dev_init(int device) {
 }
 
 OB2_API int ob2_dev_count(int *n) { return rc(cudaGetDeviceCount(n)); }
+OB2_API int ob2_dev_sm_count(int *n) {
+  *n = g_sms;
+  return 0;
+}
 OB2_API void *ob2_dev_stream(void) { return (void *)g_stream; }
 OB2_API int ob2_dev_set_stream(void *s) {
   g_stream = s ? (cudaStream_t)s : g_default;

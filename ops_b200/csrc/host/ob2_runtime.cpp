@@ -71,6 +71,7 @@ struct Runtime {
   std::unordered_map<std::string, int> kindex;
   int block_x = 32, block_y = 4, block_z = 1;
   int device = 0;
+  int sms = 148;
   // reduction scratch: per-CTA partials + finish counter
   void *partials = nullptr;
   size_t partials_cap = 0;
@@ -280,11 +281,13 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   }
   const char *e;
   if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
+  if ((e = getenv("OPS_B200_BLOCK"))) sscanf(e, "%d,%d,%d", &r.block_x, &r.block_y, &r.block_z);
   if (r.block_x < 1) r.block_x = 32;
   if (r.block_y < 1) r.block_y = 1;
   if (r.block_z < 1) r.block_z = 1;
   if (r.initialised) return;
   check(ob2_dev_init(r.device), "ops_init (no usable CUDA device)");
+  check(ob2_dev_sm_count(&r.sms), "ops_init");
   check(ob2_dev_malloc((void **)&r.counter, 4096), "ops_init");
   check(ob2_dev_memset(r.counter, 0, 4096), "ops_init");
   r.initialised = true;
@@ -847,8 +850,31 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   }
   // scratch for per-CTA partials (grid = ceil(n/block) per axis); each
   // reduction argument's region is rounded up to 256 bytes by the stub
-  long long nblk = 1;
-  for (int i = 0; i < 3; i++) nblk *= (L->n[i] + L->block[i] - 1) / L->block[i];
+  // grid: x covers the range; y and z are capped so that the grid is about
+  // one wave of resident CTAs (SMs x CTAs per SM), threads loop over the rest
+  {
+    long long tpb = (long long)L->block[0] * L->block[1] * L->block[2];
+    long long per_sm = std::max(1LL, 2048 / tpb);
+    long long target = (long long)r.sms * per_sm;
+    long long gx = (L->n[0] + L->block[0] - 1) / L->block[0];
+    long long gy = (L->n[1] + L->block[1] - 1) / L->block[1];
+    long long gz = (L->n[2] + L->block[2] - 1) / L->block[2];
+    if (nred > 0) {  // reduction kernels stride over y/z (see the generated kernel)
+      long long cy = std::max(1LL, target / std::max(1LL, gx));
+      if (gy > cy) gy = cy;
+      long long cz = std::max(1LL, target / std::max(1LL, gx * gy));
+      if (gz > cz) gz = cz;
+    }
+    if (nred == 0 && (gy > 65535 || gz > 65535))
+      throw OPSException(OPS_NOT_IMPLEMENTED,
+                         "Error: ops_par_loop range too large along y or z for one launch");
+    if (gz > 65535) gz = 65535;
+    if (gy > 65535) gy = 65535;
+    L->grid[0] = (int)gx;
+    L->grid[1] = (int)gy;
+    L->grid[2] = (int)gz;
+  }
+  long long nblk = (long long)L->grid[0] * L->grid[1] * L->grid[2];
   size_t need = red_bytes * (size_t)nblk + 256 * (size_t)nred;
   if (need > r.partials_cap) {
     if (r.partials) {
@@ -870,6 +896,17 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
     ob2_event_record(L->ev_start);
   }
   return 1;
+}
+
+OPS_API int ob2_args_alias(const ops_arg *args, int nargs) {
+  for (int i = 0; i < nargs; i++) {
+    if (args[i].argtype != OPS_ARG_DAT || !args[i].opt || !args[i].dat) continue;
+    for (int j = i + 1; j < nargs; j++) {
+      if (args[j].argtype != OPS_ARG_DAT || !args[j].opt || args[j].dat != args[i].dat) continue;
+      if (args[i].acc != OPS_READ || args[j].acc != OPS_READ) return 1;
+    }
+  }
+  return 0;
 }
 
 OPS_API void ob2_loop_check_launch(ob2_loop *L) {
@@ -1071,6 +1108,20 @@ OPS_API void ops_print_dat_to_txtfile(ops_dat d, const char *file) {
     if ((i + 1) % (size_t)(d->size[0] * d->dim) == 0) fprintf(f, "\n");
   }
   fclose(f);
+}
+static void no_hdf5(const char *what, const char *file) {
+  fprintf(stderr, "OPS B200 backend: %s(%s) skipped: built without HDF5\n", what,
+          file ? file : "");
+}
+OPS_API void ops_fetch_dat_hdf5_file(ops_dat, char const *f) { no_hdf5("ops_fetch_dat_hdf5_file", f); }
+OPS_API void ops_fetch_block_hdf5_file(ops_block, char const *f) {
+  no_hdf5("ops_fetch_block_hdf5_file", f);
+}
+OPS_API void ops_fetch_stencil_hdf5_file(ops_stencil, char const *f) {
+  no_hdf5("ops_fetch_stencil_hdf5_file", f);
+}
+OPS_API void ops_fetch_halo_hdf5_file(ops_halo, char const *f) {
+  no_hdf5("ops_fetch_halo_hdf5_file", f);
 }
 OPS_API void ops_print_dat_to_txtfile_core(ops_dat d, const char *file) {
   ops_print_dat_to_txtfile(d, file);

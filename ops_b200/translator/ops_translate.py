@@ -555,33 +555,64 @@ class Translator:
                 w("  %s *r%d; %s *part%d; int first%d;" % (p.base_type, i, p.base_type, i, i))
                 reds.append((i, a, p))
         w("};")
+        # Point function, in two variants: with __restrict__ dat pointers
+        # (the common case: no dat is both written and passed twice, so the
+        # compiler may batch every load of the point ahead of its stores) and
+        # without (aliasing arguments).
+        I = "ob2i_" + loop.stub[len("ops_par_loop_"):]
+        dats = [(i, a, p) for i, (a, p) in enumerate(zip(loop.args, kd.params)) if a.kind == "dat"]
+        for variant, qual in (("R", "__restrict__ "), ("A", "")):
+            prm = "".join(", %s *%sq%d" % (p.base_type, qual, i) for i, a, p in dats)
+            prm += "".join(", %s *red%d" % (p.base_type, i) for i, a, p in reds)
+            w("static __device__ __forceinline__ void %s_%s(const %s &p, int x, int y, int z%s) {" %
+              (I, variant, P, prm))
+            call = []
+            for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+                if a.kind == "dat":
+                    ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
+                    w("  ACC<%s> a%d(q%d ? q%d + x * p.wx%d + y * p.wy%d + z * p.wz%d : "
+                      "(%s *)0, %s, p.ey%d, p.ez%d, p.ed%d);" %
+                      (p.base_type, i, i, i, i, i, i, p.base_type, ex, i, i, i))
+                    call.append("a%d" % i)
+                elif a.kind == "gbl":
+                    call.append("(%s *)p.g%d" % (p.base_type, i))
+                elif a.kind == "reduce":
+                    call.append("red%d" % i)
+                elif a.kind == "idx":
+                    call.append("idx")
+            if any(a.kind == "idx" for a in loop.args):
+                w("  int idx[3] = {x, y, z};")
+            w("  %s(%s);" % (loop.kernel, ", ".join(call)))
+            w("}")
+        w("template <bool RESTRICT>")
         w("__global__ void __launch_bounds__(512) %s(const __grid_constant__ %s p) {" % (K, P))
         w("  const int x = p.lo0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);")
-        w("  const int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);")
-        w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
         for i, a, p in reds:
             w("  %s red%d[%s];" % (p.base_type, i, a.dim))
             w("  for (int d = 0; d < (%s); d++) red%d[d] = ob2::identity<%s, %s>();" %
               (a.dim, i, p.base_type, a.acc))
-        w("  if (x < p.hi0 && y < p.hi1 && z < p.hi2) {")
-        call = []
-        for i, (a, p) in enumerate(zip(loop.args, kd.params)):
-            if a.kind == "dat":
-                ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
-                w("    ACC<%s> a%d(p.b%d ? p.b%d + x * p.wx%d + y * p.wy%d + z * p.wz%d : "
-                  "(%s *)0, %s, p.ey%d, p.ez%d, p.ed%d);" %
-                  (p.base_type, i, i, i, i, i, i, p.base_type, ex, i, i, i))
-                call.append("a%d" % i)
-            elif a.kind == "gbl":
-                call.append("(%s *)p.g%d" % (p.base_type, i))
-            elif a.kind == "reduce":
-                call.append("red%d" % i)
-            elif a.kind == "idx":
-                call.append("idx")
-        if any(a.kind == "idx" for a in loop.args):
-            w("    int idx[3] = {x, y, z};")
-        w("    %s(%s);" % (loop.kernel, ", ".join(call)))
-        w("  }")
+        args_call = "".join(", p.b%d" % i for i, a, p in dats) + \
+            "".join(", red%d" % i for i, a, p in reds)
+        if reds:
+            # reductions: grid of about one wave of resident CTAs, threads
+            # stride over y and z, so that few per-CTA partials are combined
+            w("  if (x < p.hi0) {")
+            w("    for (int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z); z < p.hi2;"
+              " z += (int)(gridDim.z * blockDim.z))")
+            w("      for (int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y); y < p.hi1;"
+              " y += (int)(gridDim.y * blockDim.y)) {")
+            w("        if (RESTRICT) %s_R(p, x, y, z%s);" % (I, args_call))
+            w("        else %s_A(p, x, y, z%s);" % (I, args_call))
+            w("      }")
+            w("  }")
+        else:
+            # one point per thread over the whole range
+            w("  const int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);")
+            w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
+            w("  if (x < p.hi0 && y < p.hi1 && z < p.hi2) {")
+            w("    if (RESTRICT) %s_R(p, x, y, z%s);" % (I, args_call))
+            w("    else %s_A(p, x, y, z%s);" % (I, args_call))
+            w("  }")
         if reds:
             w("  __shared__ double ob2_sh_raw[32 * 2];")
             w("  __shared__ int ob2_flag;")
@@ -612,8 +643,7 @@ class Translator:
         w("  p.hi0 = L.hi[0]; p.hi1 = L.hi[1]; p.hi2 = L.hi[2];")
         w("  p.counter = L.counter;")
         w("  dim3 blk(L.block[0], L.block[1], L.block[2]);")
-        w("  dim3 grd((L.n[0] + blk.x - 1) / blk.x, (L.n[1] + blk.y - 1) / blk.y,"
-          " (L.n[2] + blk.z - 1) / blk.z);")
+        w("  dim3 grd(L.grid[0], L.grid[1], L.grid[2]);")
         if reds:
             w("  size_t nblk = (size_t)grd.x * grd.y * grd.z;")
             w("  char *scratch = (char *)L.partials;")
@@ -635,7 +665,10 @@ class Translator:
                 w("  p.part%d = (%s *)scratch;"
                   " scratch += ((nblk * (%s) * sizeof(%s) + 255) / 256) * 256;" %
                   (i, p.base_type, a.dim, p.base_type))
-        w("  %s<<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
+        w("  if (ob2_args_alias(args, %d))" % na)
+        w("    %s<false><<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
+        w("  else")
+        w("    %s<true><<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
         w("  ob2_loop_check_launch(&L);")
         w("  ob2_loop_end(&L);")
         w("}")

@@ -560,6 +560,10 @@ OPS_API void ops_print_dat_to_txtfile(ops_dat d, const char *file) {
   fclose(f);
 }
 
+OPS_API void ops_fetch_dat_hdf5_file(ops_dat, char const *) {}
+OPS_API void ops_fetch_block_hdf5_file(ops_block, char const *) {}
+OPS_API void ops_fetch_stencil_hdf5_file(ops_stencil, char const *) {}
+OPS_API void ops_fetch_halo_hdf5_file(ops_halo, char const *) {}
 OPS_API void ops_print_dat_to_txtfile_core(ops_dat d, const char *file) {
   ops_print_dat_to_txtfile(d, file);
 }

@@ -1,0 +1,95 @@
+"""Helpers for tests: build and run application flavours, parse their output.
+
+The b200 and oracle flavours run as shared libraries loaded by a child Python
+process (apps/run_shared.py), so the backend library is loaded by a Python
+process; each run is its own process because OPS state is process-global.
+"""
+
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def ensure(name: str, flavour: str, shared: bool = True) -> str:
+    from apps import catalog
+    path = catalog.artifact(name, flavour, shared)
+    if os.path.exists(path):
+        return path
+    if not catalog.available(name):
+        pytest.skip("%s/%s not built and its sources are not present" % (name, flavour))
+    return catalog.build(name, flavour, shared=shared)
+
+
+def run_app(name: str, flavour: str, args=(), dump: bool = False, cwd=None, timeout=900):
+    """Returns (stdout, dump_path or None)."""
+    ensure(name, flavour, shared=True)
+    env = dict(os.environ)
+    dpath = None
+    if dump:
+        fd, dpath = tempfile.mkstemp(prefix="%s_%s_" % (name, flavour), suffix=".dump")
+        os.close(fd)
+        env["OPS_DUMP_FILE"] = dpath
+    r = subprocess.run([sys.executable, "-m", "apps.run_shared", name, flavour, *args],
+                       cwd=cwd or ROOT, env=dict(env, PYTHONPATH=ROOT), capture_output=True,
+                       text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise AssertionError("%s/%s failed (rc %d):\n%s\n%s" % (name, flavour, r.returncode,
+                                                                 r.stdout[-3000:], r.stderr[-3000:]))
+    return r.stdout, dpath
+
+
+def run_exe(name: str, flavour: str, args=(), cwd=None, timeout=900):
+    exe = ensure(name, flavour, shared=False)
+    r = subprocess.run([exe, *args], cwd=cwd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise AssertionError("%s/%s failed (rc %d):\n%s" % (name, flavour, r.returncode,
+                                                             r.stderr[-3000:]))
+    return r.stdout
+
+
+def result_lines(text: str, keys=("sweep", "checksum", "sums", "min", "max", "count",
+                                  "fetch_b", "fp64", "fp32")):
+    return [l for l in text.splitlines() if l.split() and l.split()[0] in keys]
+
+
+def floats(line: str):
+    return [float(x) for x in re.findall(r"-?\d+\.\d+(?:e[-+]\d+)?|-?\d+e[-+]\d+", line)]
+
+
+def assert_lines_close(got, want, rtol):
+    assert len(got) == len(want), (got, want)
+    for g, w in zip(got, want):
+        assert g.split()[0] == w.split()[0], (g, w)
+        fg, fw = floats(g), floats(w)
+        assert len(fg) == len(fw), (g, w)
+        for a, b in zip(fg, fw):
+            assert abs(a - b) <= rtol * max(abs(b), 1e-300), (g, w, abs(a - b) / max(abs(b), 1e-300))
+
+
+def clover_deck_test1() -> str:
+    """CloverLeaf test problem 1 (the reference's default deck parameters,
+    field_summary.cpp:91): 10 x 2 cells on a 10 x 2 domain, a dense region
+    over x in [0,5], run to t = 3.0."""
+    return ("*clover\n state 1 density=0.2 energy=1.0\n"
+            " state 2 density=1.0 energy=2.5 geometry=rectangle xmin=0.0 xmax=5.0 ymin=0.0 "
+            "ymax=2.0\n x_cells=10\n y_cells=2\n xmin=0.0\n ymin=0.0\n xmax=10.0\n ymax=2.0\n"
+            " initial_timestep=0.04\n timestep_rise=1.5\n max_timestep=0.04\n end_time=3.0\n"
+            " test_problem 1\n*endclover\n")
+
+
+def clover_deck_test2() -> str:
+    """CloverLeaf test problem 2 (field_summary.cpp:92): 960 x 960 cells on a
+    10 x 10 domain, 87 steps."""
+    return ("*clover\n state 1 density=0.2 energy=1.0\n"
+            " state 2 density=1.0 energy=2.5 geometry=rectangle xmin=0.0 xmax=5.0 ymin=0.0 "
+            "ymax=2.0\n x_cells=960\n y_cells=960\n xmin=0.0\n ymin=0.0\n xmax=10.0\n ymax=10.0\n"
+            " initial_timestep=0.04\n timestep_rise=1.5\n max_timestep=0.04\n end_step=87\n"
+            " test_problem 2\n*endclover\n")

@@ -1,0 +1,128 @@
+"""GPU parity of whole OPS programs: the b200 build against the CPU oracle on
+the same inputs, dat by dat (halos included), and the reference's known
+answers on the b200 build.
+
+Tolerances: integer dats bit-exact; FP64 dats 1e-12 relative per element
+(the generated kernels use IEEE arithmetic without FMA contraction, so in
+practice they are bit-identical); reductions 1e-11 relative; FP32-storage dats
+1e-6 relative (one float rounding of an FP64 value that was computed in a
+different order).
+"""
+
+import os
+import re
+import tempfile
+
+import pytest
+
+from tests.apprun import (assert_lines_close, clover_deck_test1, clover_deck_test2,
+                          result_lines, run_app, run_exe)
+from tests.opsdump import compare
+
+pytestmark = pytest.mark.gpu
+
+
+def check_dumps(gpu_dump, cpu_dump, tol=1e-12, float_tol=1e-6, skip=()):
+    from tests.opsdump import read_dump
+    diffs = compare(gpu_dump, cpu_dump, skip=skip)
+    meta = read_dump(cpu_dump)
+    bad = {}
+    for name, d in diffs.items():
+        t = float_tol if meta[name][0]["type"] == "float" else tol
+        if d > t:
+            bad[name] = d
+    assert not bad, bad
+    return diffs
+
+
+@pytest.mark.parametrize("args", [[], ["-nx=29", "-ny=17"], ["-nx=130", "-ny=7"]])
+def test_opsunit_parity(args, golden):
+    gout, gd = run_app("opsunit", "b200", args, dump=True)
+    cout, cd = run_app("opsunit", "oracle", args, dump=True)
+    check_dumps(gd, cd)
+    assert_lines_close(result_lines(gout), result_lines(cout), 1e-11)
+    if not args:
+        want = golden["reference_runs"]["opsunit_default"]["lines"]
+        got = [l for l in result_lines(gout) if l.split()[0] in ("sums", "min", "max", "count",
+                                                                  "fetch_b")]
+        assert_lines_close(got, want, 1e-11)
+
+
+def test_poisson_mb_parity_and_reference(golden):
+    gout, gd = run_app("poisson_mb", "b200", dump=True)
+    cout, cd = run_app("poisson_mb", "oracle", dump=True)
+    check_dumps(gd, cd)
+    want = golden["reference_runs"]["poisson_mb_default"]["lines"]
+    assert_lines_close(result_lines(gout), want, 1e-11)
+
+
+def test_poisson_mb_3x3_ragged(golden):
+    g = golden["reference_runs"]["poisson_mb_3x3"]
+    gout, gd = run_app("poisson_mb", "b200", g["args"], dump=True)
+    cout, cd = run_app("poisson_mb", "oracle", g["args"], dump=True)
+    check_dumps(gd, cd)
+    assert_lines_close(result_lines(gout), g["lines"], 1e-11)
+
+
+@pytest.mark.parametrize("args", [["-n=24", "-steps=5", "-prec=both"],
+                                  ["-nx=33", "-ny=17", "-nz=20", "-steps=3", "-prec=both"],
+                                  ["-nx=300", "-ny=9", "-nz=6", "-steps=2", "-prec=64"]])
+def test_adi3d_parity(args):
+    gout, gd = run_app("adi3d", "b200", args, dump=True)
+    cout, cd = run_app("adi3d", "oracle", args, dump=True)
+    check_dumps(gd, cd, tol=1e-12, float_tol=1e-6)
+    assert_lines_close(result_lines(gout, ("fp64",))[:1], result_lines(cout, ("fp64",))[:1], 1e-11)
+
+
+def test_cloverleaf_fields_match_oracle(tmp_path):
+    import json
+    import subprocess
+    import sys
+    from tests.apprun import ensure, ROOT
+    ensure("clover_step", "b200")
+    ensure("clover_step", "oracle")
+    dumps = {}
+    for fl in ("b200", "oracle"):
+        dumps[fl] = str(tmp_path / ("%s.dump" % fl))
+        r = subprocess.run([sys.executable, "-m", "apps.clover_run", "--flavour", fl, "--cells",
+                            "96", "--steps", "15", "--dump", dumps[fl]], cwd=ROOT,
+                           capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+    check_dumps(dumps["b200"], dumps["oracle"])
+
+
+def test_reference_poisson_on_b200(golden):
+    out = run_exe("ref_poisson", "b200")
+    v = float(re.search(r"Total error: (\S+)", out).group(1))
+    want = golden["known_answers"]["ref_poisson_default_total_error"]["value"]
+    assert abs(v - want) <= 1e-12 * want and "PASSED" in out
+
+
+def test_reference_laplace_on_b200(golden):
+    out = run_exe("ref_laplace", "b200")
+    assert "PASSED" in out, out[-500:]
+
+
+@pytest.mark.parametrize("deck", ["test1", "test2"])
+def test_reference_cloverleaf_known_answers_on_b200(deck):
+    d = tempfile.mkdtemp(prefix="clover_%s_" % deck)
+    with open(os.path.join(d, "clover.in"), "w") as f:
+        f.write(clover_deck_test1() if deck == "test1" else clover_deck_test2())
+    out = run_exe("cloverleaf", "b200", cwd=d)
+    assert "This test is considered PASSED" in out, out[-800:]
+
+
+def test_reference_mblock_halos_match_oracle(tmp_path):
+    """mblock (reference app): multi-block halo transfers with flipped and
+    permuted orientations; every dat compared with the oracle."""
+    import subprocess
+    from tests.apprun import ensure
+    dumps = {}
+    for fl in ("b200", "oracle"):
+        exe = ensure("ref_mblock", fl, shared=False)
+        dumps[fl] = str(tmp_path / ("%s.dump" % fl))
+        r = subprocess.run([exe], cwd=str(tmp_path), capture_output=True, text=True,
+                           env=dict(os.environ, OPS_DUMP_FILE=dumps[fl]), timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+    diffs = compare(dumps["b200"], dumps["oracle"])
+    assert max(diffs.values()) == 0.0, diffs

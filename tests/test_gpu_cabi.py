@@ -1,0 +1,161 @@
+"""The halo-transfer and batched-tridiagonal kernels driven through the C ABI
+from this Python process (libops_b200.so loaded here), checked against numpy
+restatements of the reference semantics.
+
+Halo transfers must be bit-exact (copies); tridiagonal solves within 1e-12
+relative (FP64) of an FP64 Thomas solve; FP32 storage within 2 float ulps.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def np_halo(src, dst, s_meta, d_meta, iters, fbase, tbase, fdir, tdir):
+    """numpy model of one halo (ops_host_singlenode.cpp:172-446 semantics) on
+    full arrays indexed [z][y][x] / [y][x]; meta = (d_m list)."""
+    nd = len(iters)
+    out = dst.copy()
+    it = np.indices(iters[::-1]).reshape(nd, -1)[::-1]  # it[a] = coordinate along axis a
+    def index(base, dirs, dm):
+        idx = []
+        for i in range(nd):
+            ax = abs(dirs[i]) - 1
+            t = it[ax] if dirs[i] > 0 else iters[ax] - 1 - it[ax]
+            idx.append(base[i] - dm[i] + t)
+        return tuple(idx[::-1])
+    out[index(tbase, tdir, d_meta)] = src[index(fbase, fdir, s_meta)].astype(dst.dtype)
+    return out
+
+
+CASES_2D = [
+    # iter, from_base, to_base, from_dir, to_dir
+    ([1, 14], [11, 0], [-1, 0], [1, 2], [1, 2]),       # x face, same orientation
+    ([12, 2], [0, 0], [0, 14], [1, 2], [1, 2]),        # 2-deep y face
+    ([1, 15], [0, 0], [20, 0], [1, 2], [1, -2]),       # flipped along y
+    ([10, 1], [2, 3], [-1, 0], [1, 2], [2, 1]),        # x of source -> y of target
+    ([6, 4], [1, 2], [-2, -2], [-1, 2], [2, -1]),      # permuted and flipped, into halo corner
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES_2D)))
+@pytest.mark.parametrize("types", [("double", "double"), ("float", "float"), ("double", "float")])
+def test_halo_transfer_2d(case, types):
+    from tests import cabi
+    L = cabi.lib()
+    b0 = L.ops_decl_block(2, b"hb0")
+    b1 = L.ops_decl_block(2, b"hb1")
+    src = cabi.Dat(b0, 2, [12, 20], [-2, -2], [2, 2], types[0], "src")
+    dst = cabi.Dat(b1, 2, [20, 14], [-2, -2], [2, 2], types[1], "dst")
+    rng = np.random.default_rng(case)
+    s = rng.standard_normal(src.full_shape()).astype(src.dtype)
+    d = rng.standard_normal(dst.full_shape()).astype(dst.dtype)
+    src.set_full(s)
+    dst.set_full(d)
+    iters, fb, tb, fd, td = CASES_2D[case]
+    h = L.ops_decl_halo(src.h, dst.h, cabi.ivec(iters), cabi.ivec(fb), cabi.ivec(tb),
+                        cabi.ivec(fd), cabi.ivec(td))
+    grp = L.ops_decl_halo_group(1, (C.c_void_p * 1)(h))
+    L.ops_halo_transfer(grp)
+    got = dst.get_full()
+    want = np_halo(s, d, src.d_m, dst.d_m, iters, fb, tb, fd, td)
+    assert np.array_equal(got, want)
+
+
+def test_halo_group_3d_many():
+    from tests import cabi
+    L = cabi.lib()
+    b = L.ops_decl_block(3, b"h3")
+    a = cabi.Dat(b, 3, [9, 7, 5], [-1, -1, -1], [1, 1, 1], "double", "a3")
+    c = cabi.Dat(b, 3, [7, 9, 6], [-1, -1, -1], [1, 1, 1], "double", "c3")
+    rng = np.random.default_rng(7)
+    sa, sc = rng.standard_normal(a.full_shape()), rng.standard_normal(c.full_shape())
+    a.set_full(sa)
+    c.set_full(sc)
+    specs = [([1, 7, 5], [8, 0, 0], [-1, 0, 0], [1, 2, 3], [1, 2, 3]),
+             ([7, 1, 5], [0, 0, 0], [0, 9, 0], [2, 1, 3], [1, 2, -3]),
+             ([9, 7, 1], [0, 0, 4], [0, 0, -1], [1, 2, 3], [2, 1, 3])]
+    hs = []
+    want = sc
+    for it, fb, tb, fd, td in specs:
+        hs.append(L.ops_decl_halo(a.h, c.h, cabi.ivec(it), cabi.ivec(fb), cabi.ivec(tb),
+                                  cabi.ivec(fd), cabi.ivec(td)))
+        want = np_halo(sa, want, a.d_m, c.d_m, it, fb, tb, fd, td)
+    grp = L.ops_decl_halo_group(len(hs), (C.c_void_p * len(hs))(*hs))
+    L.ops_halo_transfer(grp)
+    assert np.array_equal(c.get_full(), want)
+
+
+def thomas(a, b, c, d):
+    n = len(d)
+    cp, dp = np.zeros(n), np.zeros(n)
+    cp[0], dp[0] = c[0] / b[0], d[0] / b[0]
+    for i in range(1, n):
+        m = 1.0 / (b[i] - a[i] * cp[i - 1])
+        cp[i], dp[i] = c[i] * m, (d[i] - a[i] * dp[i - 1]) * m
+    for i in range(n - 2, -1, -1):
+        dp[i] -= cp[i] * dp[i + 1]
+    return dp
+
+
+def np_trid(A, B, Cc, D, U, solvedim, rng_box):
+    """solve along axis solvedim (0=x) of [z][y][x] arrays inside the box"""
+    X = D.copy() if U is None else U.copy()
+    axis = 2 - solvedim
+    sl = tuple(slice(rng_box[2 * (2 - k)], rng_box[2 * (2 - k) + 1]) for k in range(3))
+    a, b, c, d = (np.moveaxis(M[sl].astype(np.float64), axis, -1) for M in (A, B, Cc, D))
+    sol = np.empty_like(d)
+    for idx in np.ndindex(d.shape[:-1]):
+        sol[idx] = thomas(a[idx], b[idx], c[idx], d[idx])
+    sol = np.moveaxis(sol, -1, axis)
+    if U is None:
+        X[sl] = sol.astype(X.dtype)
+    else:
+        X[sl] = (X[sl].astype(np.float64) + sol).astype(X.dtype)
+    return X
+
+
+@pytest.mark.parametrize("typ", ["double", "float"])
+@pytest.mark.parametrize("solvedim", [0, 1, 2])
+@pytest.mark.parametrize("inc", [False, True])
+@pytest.mark.parametrize("shape", [(33, 7, 5), (7, 40, 3), (5, 6, 300), (1, 4, 3)])
+def test_trid_batch(typ, solvedim, inc, shape):
+    from tests import cabi
+    L = cabi.lib()
+    blk = L.ops_decl_block(3, b"trid")
+    nx, ny, nz = shape
+    dats = {k: cabi.Dat(blk, 3, [nx, ny, nz], [-1, -1, -1], [1, 1, 1], typ, k)
+            for k in "abcdu"}
+    rng = np.random.default_rng(hash((typ, solvedim, inc, shape)) & 0xffff)
+    full = dats["a"].full_shape()
+    vals = {"a": rng.uniform(-1, 1, full), "c": rng.uniform(-1, 1, full),
+            "b": 3.0 + rng.uniform(0, 1, full), "d": rng.uniform(-1, 1, full),
+            "u": rng.uniform(-1, 1, full)}
+    for k in "abcdu":
+        vals[k] = vals[k].astype(dats[k].dtype)
+        dats[k].set_full(vals[k])
+    box = [0, nx, 0, ny, 0, nz]
+    if nx > 3 and ny > 3:
+        box = [1, nx - 1, 2, ny, 0, nz]  # a sub-range
+    r = cabi.ivec(box)
+    if inc:
+        L.ops_tridMultiDimBatch_Inc(3, solvedim, r, dats["a"].h, dats["b"].h, dats["c"].h,
+                                    dats["d"].h, dats["u"].h, None)
+        got, target = dats["u"].get_full(), "u"
+    else:
+        L.ops_tridMultiDimBatch(3, solvedim, r, dats["a"].h, dats["b"].h, dats["c"].h,
+                                dats["d"].h, None)
+        got, target = dats["d"].get_full(), "d"
+    # the storage box of the range: halo offset 1 in every axis
+    sbox = [box[0] + 1, box[1] + 1, box[2] + 1, box[3] + 1, box[4] + 1, box[5] + 1]
+    want = np_trid(vals["a"], vals["b"], vals["c"], vals["d"], vals["u"] if inc else None,
+                   solvedim, sbox)
+    if typ == "double":
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-13)
+    else:
+        np.testing.assert_allclose(got, want, rtol=2.5e-7, atol=1e-6)
+    if inc:  # d untouched by the _Inc form
+        assert np.array_equal(dats["d"].get_full(), vals["d"])

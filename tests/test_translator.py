@@ -1,0 +1,82 @@
+"""Translator unit tests (CPU only): parsing, generated code, compilation."""
+
+import os
+import subprocess
+import tempfile
+
+import pytest
+
+from ops_b200.translator.ops_translate import (Translator, find_calls, mask_comments_strings,
+                                               parse_arg, parse_params, top_level_functions)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_mask_keeps_offsets():
+    src = 'a(1) /* b(2) */ "c(3)" // d(4)\nx'
+    m = mask_comments_strings(src)
+    assert len(m) == len(src) and m.endswith("\nx") and "b(2)" not in m and "c(3)" not in m
+
+
+def test_find_calls_nested_and_comments():
+    src = ('ops_par_loop(k, "n", blk, 2, r, ops_arg_dat(d, 1, S, "double", OPS_READ), f(g(1), 2));'
+           '\n// ops_par_loop(commented, x)\n')
+    calls = find_calls(src, "ops_par_loop")
+    assert len(calls) == 1
+    args = calls[0][2]
+    assert args[0] == "k" and args[5].startswith("ops_arg_dat") and args[6] == "f(g(1), 2)"
+
+
+def test_parse_args_kinds():
+    a = parse_arg('ops_arg_dat(u[i+ngrid*j], 1, S2D_00, "double", OPS_READ)', "t")
+    assert (a.kind, a.ctype, a.dim, a.acc) == ("dat", "double", "1", "OPS_READ")
+    a = parse_arg('ops_arg_dat_opt(o, 3, S, "float", OPS_WRITE, flag)', "t")
+    assert a.kind == "dat" and a.opt and a.dim == "3"
+    a = parse_arg('ops_arg_gbl(fields, NUM_FIELDS, "int", OPS_READ)', "t")
+    assert (a.kind, a.dim) == ("gbl", "NUM_FIELDS")
+    a = parse_arg('ops_arg_reduce(h, 2, "double", OPS_MIN)', "t")
+    assert (a.kind, a.acc) == ("reduce", "OPS_MIN")
+    assert parse_arg("ops_arg_idx()", "t").kind == "idx"
+    with pytest.raises(SystemExit):
+        parse_arg('ops_arg_gbl(x, 1, "double", OPS_INC)', "t")
+
+
+def test_parse_params():
+    ps = parse_params("const ACC<double> &u, ACC<float>& v, const int *idx, double* r")
+    assert [p.is_acc for p in ps] == [True, True, False, False]
+    assert [p.base_type for p in ps] == ["double", "float", "int", "double"]
+
+
+def test_top_level_functions_skip_structs_and_comments():
+    text = ("#include \"x.h\"\nstruct S { int a; };\n"
+            "void k1(const ACC<double> &u /* note */, double *r) { *r += u(0,0); }\n"
+            "static inline double helper(double a) { return a * 2; }\n")
+    fs = {f.name: f for f in top_level_functions(text, "h")}
+    assert set(fs) == {"k1", "helper"}
+    assert fs["k1"].params is not None and len(fs["k1"].params) == 2
+
+
+def test_translate_and_compile_opsunit():
+    out = tempfile.mkdtemp(prefix="tr_")
+    src = os.path.join(ROOT, "apps", "opsunit", "opsunit.cpp")
+    Translator([src], [], "opsunit", out).run()
+    cu = open(os.path.join(out, "opsunit_kernels.cu")).read()
+    # one kernel per loop signature, both aliasing variants, restrict pointers
+    for k in ("ou_fill", "ou_vec", "ou_stencil", "ou_strided", "ou_reduce", "ou_opt", "ou_rw",
+              "ou_colsum"):
+        assert "ob2k_%s(" % k in cu
+        assert "ob2i_%s_R" % k in cu and "ob2i_%s_A" % k in cu
+    assert "__restrict__" in cu and "__constant__ double ou_scale;" in cu
+    assert "ob2::final_combine<double, OPS_MIN>" in cu
+    ops = open(os.path.join(out, "opsunit_ops.cpp")).read()
+    assert "ops_par_loop(" not in ops.replace("ops_par_loop_", "")
+    # compile the kernels for sm_100a (cross-compiles without a GPU)
+    nvcc = "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not present")
+    r = subprocess.run([nvcc, "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-w",
+                        "--fmad=false", "-I" + os.path.join(ROOT, "include"),
+                        "-I" + os.path.join(ROOT, "apps", "opsunit"), "-c",
+                        os.path.join(out, "opsunit_kernels.cu"), "-o",
+                        os.path.join(out, "k.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
