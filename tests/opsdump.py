@@ -45,9 +45,10 @@ def read_dump(path: str) -> Dict[str, Tuple[dict, np.ndarray]]:
 
 
 def compare(a_path: str, b_path: str, rtol: float = 1e-12, exact_types=("int",),
-            skip=()) -> Dict[str, float]:
-    """Max relative difference per dat (|a-b| / max(|b|, floor)); raises on
-    shape/type mismatch.  Integer dats must match exactly."""
+            skip=(), floor_frac: float = 1e-3) -> Dict[str, float]:
+    """Max relative difference per dat, |a-b| / max(|b|, floor_frac * max|b|);
+    floor_frac = 1 gives the error relative to the field's scale.  Raises on
+    shape/type mismatch; integer dats must match exactly."""
     A, Bd = read_dump(a_path), read_dump(b_path)
     assert set(A) == set(Bd), "dat sets differ: %s" % (set(A) ^ set(Bd))
     res = {}
@@ -65,6 +66,6 @@ def compare(a_path: str, b_path: str, rtol: float = 1e-12, exact_types=("int",),
         scale = max(float(np.max(np.abs(xb))) if xb.size else 0.0, 1e-300)
         diff = np.abs(xa - xb)
         # per element relative with an absolute floor relative to the field scale
-        rel = diff / np.maximum(np.abs(xb), 1e-3 * scale)
+        rel = diff / np.maximum(np.abs(xb), floor_frac * scale)
         res[name] = float(np.max(rel)) if rel.size else 0.0
     return res

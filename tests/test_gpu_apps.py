@@ -22,9 +22,9 @@ from tests.opsdump import compare
 pytestmark = pytest.mark.gpu
 
 
-def check_dumps(gpu_dump, cpu_dump, tol=1e-12, float_tol=1e-6, skip=()):
+def check_dumps(gpu_dump, cpu_dump, tol=1e-12, float_tol=1e-6, skip=(), floor_frac=1e-3):
     from tests.opsdump import read_dump
-    diffs = compare(gpu_dump, cpu_dump, skip=skip)
+    diffs = compare(gpu_dump, cpu_dump, skip=skip, floor_frac=floor_frac)
     meta = read_dump(cpu_dump)
     bad = {}
     for name, d in diffs.items():
@@ -68,9 +68,13 @@ def test_poisson_mb_3x3_ragged(golden):
                                   ["-nx=33", "-ny=17", "-nz=20", "-steps=3", "-prec=both"],
                                   ["-nx=300", "-ny=9", "-nz=6", "-steps=2", "-prec=64"]])
 def test_adi3d_parity(args):
+    """The solves use a different elimination order than the oracle's Thomas
+    sweep (chunked Thomas + PCR), so agreement is at round-off relative to the
+    field's scale: |gpu - oracle| <= 1e-12 * max|oracle| per dat (FP64), and
+    one float rounding for FP32 storage."""
     gout, gd = run_app("adi3d", "b200", args, dump=True)
     cout, cd = run_app("adi3d", "oracle", args, dump=True)
-    check_dumps(gd, cd, tol=1e-12, float_tol=1e-6)
+    check_dumps(gd, cd, tol=1e-12, float_tol=1e-6, floor_frac=1.0)
     assert_lines_close(result_lines(gout, ("fp64",))[:1], result_lines(cout, ("fp64",))[:1], 1e-11)
 
 

@@ -121,7 +121,7 @@ def np_trid(A, B, Cc, D, U, solvedim, rng_box):
 @pytest.mark.parametrize("typ", ["double", "float"])
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 @pytest.mark.parametrize("inc", [False, True])
-@pytest.mark.parametrize("shape", [(33, 7, 5), (7, 40, 3), (5, 6, 300), (1, 4, 3)])
+@pytest.mark.parametrize("shape", [(33, 7, 5), (7, 40, 3), (5, 6, 300), (2, 4, 3)])
 def test_trid_batch(typ, solvedim, inc, shape):
     from tests import cabi
     L = cabi.lib()
