@@ -186,6 +186,7 @@ int main(int argc, char **argv) {
   delete ctx_x;
   delete ctx_y;
   delete ctx_z;
+  ops_timing_output(std::cout);
   ops_exit();
   return 0;
 }

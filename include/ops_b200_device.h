@@ -73,6 +73,33 @@ typedef struct ob2_halo_task {
 /* tasks: device array of ntasks entries; max_pts: largest npts */
 OB2_API int ob2_halo_run(const ob2_halo_task *tasks_dev, int ntasks, long long max_pts);
 
+/* Halo transfer that allocates nothing (no counterpart in the reference).
+ *
+ * For callers that must not call cudaMalloc: code that runs while another
+ * component owns the device memory budget (a serving process whose pool is
+ * carved up in advance, a framework's caching allocator), or host code that
+ * may not create allocations between setup and teardown.  ob2_halo_run needs
+ * its task table in device memory that the caller allocated; this variant
+ * takes the table in host memory and stages it, with an ordinary stream-
+ * ordered copy, into a fixed array of OB2_HALO_STATIC_MAX tasks that is
+ * compiled into the library (a file-scope __device__ array: every GPU that
+ * loads the library holds its OB2_HALO_STATIC_MAX x sizeof(ob2_halo_task),
+ * about 210 KB, until the process exits).  The halo
+ * kernel itself is the same as ob2_halo_run's.
+ *
+ * - Returns OB2_ERR_NOALLOC_LIMIT (see ob2_error_string) when ntasks exceeds
+ *   OB2_HALO_STATIC_MAX, without copying or launching anything.
+ * - The first call on a device looks up the array's device address on that
+ *   device (cudaGetSymbolAddress); make that first call before any stream
+ *   capture begins.
+ * - All calls share the one array, which keeps the last call's table: two
+ *   calls whose work overlaps on the GPU (different streams, or different
+ *   host threads) race on it.  Calls on one stream are ordered and safe.
+ * - Calls no cudaMalloc / cudaFree and no allocating library routine. */
+#define OB2_HALO_STATIC_MAX 1024
+#define OB2_ERR_NOALLOC_LIMIT 100001
+OB2_API int ob2_halo_run_noalloc(const ob2_halo_task *tasks_host, int ntasks);
+
 /* ---- dense box copy between a dat and a packed AoS buffer
  *      (ops_cuda_rt_support.cu:256-451, fetch/set slab).  dir 0: dat->buf,
  *      dir 1: buf->dat.  buf may be device or host-pinned memory. ---- */

@@ -76,7 +76,11 @@ OB2_API int ob2_host_alloc_pinned(void **p, size_t n) {
   return rc(cudaHostAlloc(p, n ? n : 16, cudaHostAllocPortable));
 }
 OB2_API int ob2_host_free_pinned(void *p) { return p ? rc(cudaFreeHost(p)) : 0; }
-OB2_API const char *ob2_error_string(int code) { return cudaGetErrorString((cudaError_t)code); }
+OB2_API const char *ob2_error_string(int code) {
+  if (code == OB2_ERR_NOALLOC_LIMIT)
+    return "halo task table larger than the allocation-free maximum (OB2_HALO_STATIC_MAX)";
+  return cudaGetErrorString((cudaError_t)code);
+}
 OB2_API int ob2_last_launch_error(void) { return rc(cudaGetLastError()); }
 OB2_API int ob2_mem_info(size_t *f, size_t *t) { return rc(cudaMemGetInfo(f, t)); }
 
@@ -163,6 +167,45 @@ OB2_API int ob2_halo_run(const ob2_halo_task *tasks_dev, int ntasks, long long m
   dim3 grid((unsigned)blocks, (unsigned)ntasks);
   halo_kernel<<<grid, 256, 0, g_stream>>>(tasks_dev);
   return rc(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free halo transfer: the task table lives in a fixed array
+// compiled into this library instead of caller-allocated device memory.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __align__(256) ob2_halo_task g_halo_static[OB2_HALO_STATIC_MAX];
+
+constexpr int kMaxDevices = 64;
+// device address of g_halo_static, looked up once per device (host code may
+// not pass the symbol itself to a kernel: its host-side name is a stand-in)
+ob2_halo_task *g_halo_static_addr[kMaxDevices] = {nullptr};
+
+}  // namespace
+
+OB2_API int ob2_halo_run_noalloc(const ob2_halo_task *tasks_host, int ntasks) {
+  if (ntasks < 0 || ntasks > OB2_HALO_STATIC_MAX) return OB2_ERR_NOALLOC_LIMIT;
+  if (ntasks == 0) return 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return rc(e);
+  if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+  if (!g_halo_static_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_halo_static);
+    if (e != cudaSuccess) return rc(e);
+    g_halo_static_addr[dev] = (ob2_halo_task *)p;
+  }
+  long long max_pts = 0;
+  for (int i = 0; i < ntasks; i++)
+    if (tasks_host[i].npts > max_pts) max_pts = tasks_host[i].npts;
+  // stream-ordered: an earlier launch on this stream still reading the table
+  // finishes before it is overwritten
+  e = cudaMemcpyAsync(g_halo_static_addr[dev], tasks_host, sizeof(ob2_halo_task) * ntasks,
+                      cudaMemcpyHostToDevice, g_stream);
+  if (e != cudaSuccess) return rc(e);
+  return ob2_halo_run(g_halo_static_addr[dev], ntasks, max_pts);
 }
 
 // ---------------------------------------------------------------------------
