@@ -54,6 +54,8 @@ typedef struct ob2_loop {
   int grid[3];              /* suggested grid: x covers the range, y/z capped
                                at about one full wave of resident CTAs; the
                                kernel loops over the remaining y/z */
+  int idx32;                /* 1: every dat has < 2^31 elements, so element
+                               offsets fit 32-bit arithmetic */
 } ob2_loop;
 
 /* Returns 0 when the range is empty (nothing to launch, ob2_loop_end not

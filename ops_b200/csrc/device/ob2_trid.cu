@@ -6,46 +6,43 @@
 // published by Laszlo, Giles and Appleyard, "Manycore algorithms for batch
 // scalar and block tridiagonal solvers", ACM TOMS 42(4), 2016):
 //
-//   * a line of n points is cut into P nearly equal chunks (lengths differ by
-//     at most one, every chunk 8..16 points when n > 16), one thread per
-//     chunk, coefficients held in FP64 registers;
+//   * a line of n points is cut into P = ceil(n/CL) chunks of CL points (the
+//     last one padded with identity rows), one thread per chunk, the chunk's
+//     coefficients held in FP64 registers;
 //   * each thread eliminates its chunk so that every row couples only to the
 //     chunk's first and last unknowns ("modified Thomas");
 //   * the chunk end rows form a tridiagonal system of 2P unknowns per line,
-//     solved by parallel cyclic reduction in shared memory;
+//     solved by parallel cyclic reduction (PCR);
 //   * each thread substitutes its chunk and writes the solution (or adds it
 //     to u for the _Inc form, leaving d untouched).
 //
-// Each coefficient is read once and the solution written once: the DRAM
-// traffic is the algorithmic 5 values per point (7 for _Inc).  For unit-stride
-// lines the P threads of a line hold adjacent chunks; for strided lines
-// neighbouring threads hold neighbouring lines, so every warp load is a
-// contiguous run along x.  Elimination is FP64 for double and float storage.
+// Lines of up to 32*CL points use one warp per line and PCR with warp
+// shuffles (no shared memory, no CTA barriers).  For strided lines (y, z)
+// the CTA's 8 lines are staged through shared memory so that loads and
+// stores are contiguous runs along x.  Longer lines use a CTA per group of
+// lines with PCR in shared memory.  Each coefficient is read once and the
+// solution written once: the DRAM traffic is the algorithmic 5 values per
+// point (7 for _Inc).  Elimination is FP64 for double and float storage.
+// Every register array is indexed with compile-time indices only (a run-time
+// index would move the arrays to local memory).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include "ops_b200_device.h"
 
 namespace {
 
-constexpr int kMaxL = 16;          // max points per chunk (registers)
-constexpr int kMaxThreads = 256;   // => max line length 4096
+constexpr int kThreads = 256;  // CTA size
 
-// After chunk_reduce, row i of a chunk of length L reads
-//   a_i * x_first + x_i + c_i * x_last = d_i        (0 < i < L-1)
+// After chunk_reduce (all CL rows; padding rows are b = 1, a = c = d = 0),
+// row i of the chunk reads
+//   a_i * x_first + x_i + c_i * x_last = d_i        (0 < i < CL-1)
 //   a_0 * x_prev  + x_0 + c_0 * x_last = d_0        (row 0)
-//   a_{L-1} * x_0 + x_{L-1} + c_{L-1} * x_next = d_{L-1}   (row L-1)
+//   a_{CL-1} * x_0 + x_{CL-1} + c_{CL-1} * x_next = d_{CL-1}   (last row)
 // where x_prev / x_next are the end unknowns of the neighbouring chunks.
-__device__ __forceinline__ void chunk_reduce(int L, double *a, double *b, double *c, double *d) {
-  if (L <= 2) {
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-      if (i < L) {
-        double r = 1.0 / b[i];
-        a[i] *= r; c[i] *= r; d[i] *= r;
-      }
-    return;
-  }
+template <int CL>
+__device__ __forceinline__ void chunk_reduce(double *a, const double *b, double *c, double *d) {
   {
     double r = 1.0 / b[0];
     a[0] *= r; c[0] *= r; d[0] *= r;
@@ -54,93 +51,236 @@ __device__ __forceinline__ void chunk_reduce(int L, double *a, double *b, double
   }
   // forward: row i (i >= 2) loses x_{i-1}, gains x_0
 #pragma unroll
-  for (int i = 2; i < kMaxL; i++)
-    if (i < L) {
-      double r = 1.0 / (b[i] - a[i] * c[i - 1]);
-      d[i] = r * (d[i] - a[i] * d[i - 1]);
-      a[i] = -r * a[i] * a[i - 1];
-      c[i] = r * c[i];
-    }
-  // backward: row i (L-3 >= i >= 1) loses x_{i+1}, gains x_{L-1}
+  for (int i = 2; i < CL; i++) {
+    const double r = 1.0 / (b[i] - a[i] * c[i - 1]);
+    d[i] = r * (d[i] - a[i] * d[i - 1]);
+    a[i] = -r * a[i] * a[i - 1];
+    c[i] = r * c[i];
+  }
+  // backward: row i (CL-3 >= i >= 1) loses x_{i+1}, gains x_{CL-1}
 #pragma unroll
-  for (int i = kMaxL - 3; i >= 1; i--)
-    if (i <= L - 3) {
-      d[i] = d[i] - c[i] * d[i + 1];
-      a[i] = a[i] - c[i] * a[i + 1];
-      c[i] = -c[i] * c[i + 1];
-    }
-  // row 0 loses x_1, gains x_{L-1}
+  for (int i = CL - 3; i >= 1; i--) {
+    d[i] = d[i] - c[i] * d[i + 1];
+    a[i] = a[i] - c[i] * a[i + 1];
+    c[i] = -c[i] * c[i + 1];
+  }
+  // row 0 loses x_1, gains x_{CL-1}
   {
-    double r = 1.0 / (1.0 - c[0] * a[1]);
+    const double r = 1.0 / (1.0 - c[0] * a[1]);
     d[0] = r * (d[0] - c[0] * d[1]);
     a[0] = r * a[0];
     c[0] = -r * c[0] * c[1];
   }
 }
 
-template <typename T, bool INC>
-__global__ void __launch_bounds__(256) trid_hybrid_kernel(
-    int n, int P, int LPB, long long nlines, int unit, long long stride, int o1n, long long o1s,
+// PCR over the 64 end unknowns of a line held two per lane (rows 2*lane and
+// 2*lane+1) with warp shuffles; returns this lane's two solutions.  Rows are
+// a x_{r-s} + x_r + c x_{r+s} = d at each stride s.
+__device__ __forceinline__ void warp_pcr(double a0, double c0, double d0, double a1, double c1,
+                                         double d1, int lane, double &xf, double &xl) {
+  const unsigned full = 0xffffffffu;
+  // s = 1: row 2p couples to 2p-1 (lane p-1, last) and 2p+1 (own last);
+  // row 2p+1 couples to 2p (own first) and 2p+2 (lane p+1, first)
+  {
+    const double pa1 = __shfl_up_sync(full, a1, 1), pc1 = __shfl_up_sync(full, c1, 1),
+                 pd1 = __shfl_up_sync(full, d1, 1);
+    const double na0 = __shfl_down_sync(full, a0, 1), nc0 = __shfl_down_sync(full, c0, 1),
+                 nd0 = __shfl_down_sync(full, d0, 1);
+    const bool hasl = lane > 0, hasr = lane < 31;
+    double k1 = hasl ? a0 : 0.0, k2 = c0;
+    double inv = 1.0 / (1.0 - k1 * (hasl ? pc1 : 0.0) - k2 * a1);
+    const double A0 = -k1 * (hasl ? pa1 : 0.0) * inv, C0 = -k2 * c1 * inv,
+                 D0 = (d0 - k1 * (hasl ? pd1 : 0.0) - k2 * d1) * inv;
+    k1 = a1;
+    k2 = hasr ? c1 : 0.0;
+    inv = 1.0 / (1.0 - k1 * c0 - k2 * (hasr ? na0 : 0.0));
+    const double A1 = -k1 * a0 * inv, C1 = -k2 * (hasr ? nc0 : 0.0) * inv,
+                 D1 = (d1 - k1 * d0 - k2 * (hasr ? nd0 : 0.0)) * inv;
+    a0 = A0; c0 = C0; d0 = D0;
+    a1 = A1; c1 = C1; d1 = D1;
+  }
+  // s = 2h rows: both rows of a lane couple to the same slot of lanes p -/+ h
+#pragma unroll
+  for (int h = 1; h < 32; h <<= 1) {
+    const bool hasl = lane >= h, hasr = lane + h < 32;
+    const double la0 = __shfl_up_sync(full, a0, h), lc0 = __shfl_up_sync(full, c0, h),
+                 ld0 = __shfl_up_sync(full, d0, h);
+    const double ra0 = __shfl_down_sync(full, a0, h), rc0 = __shfl_down_sync(full, c0, h),
+                 rd0 = __shfl_down_sync(full, d0, h);
+    const double la1 = __shfl_up_sync(full, a1, h), lc1 = __shfl_up_sync(full, c1, h),
+                 ld1 = __shfl_up_sync(full, d1, h);
+    const double ra1 = __shfl_down_sync(full, a1, h), rc1 = __shfl_down_sync(full, c1, h),
+                 rd1 = __shfl_down_sync(full, d1, h);
+    {
+      const double k1 = hasl ? a0 : 0.0, k2 = hasr ? c0 : 0.0;
+      const double inv = 1.0 / (1.0 - k1 * (hasl ? lc0 : 0.0) - k2 * (hasr ? ra0 : 0.0));
+      const double nA = -k1 * (hasl ? la0 : 0.0) * inv, nC = -k2 * (hasr ? rc0 : 0.0) * inv;
+      d0 = (d0 - k1 * (hasl ? ld0 : 0.0) - k2 * (hasr ? rd0 : 0.0)) * inv;
+      a0 = nA; c0 = nC;
+    }
+    {
+      const double k1 = hasl ? a1 : 0.0, k2 = hasr ? c1 : 0.0;
+      const double inv = 1.0 / (1.0 - k1 * (hasl ? lc1 : 0.0) - k2 * (hasr ? ra1 : 0.0));
+      const double nA = -k1 * (hasl ? la1 : 0.0) * inv, nC = -k2 * (hasr ? rc1 : 0.0) * inv;
+      d1 = (d1 - k1 * (hasl ? ld1 : 0.0) - k2 * (hasr ? rd1 : 0.0)) * inv;
+      a1 = nA; c1 = nC;
+    }
+  }
+  xf = d0;
+  xl = d1;
+}
+
+// Warp-per-line form (n <= 32*CL): lane p holds chunk p; lanes past the last
+// chunk carry identity rows.
+template <typename T, bool INC, int CL>
+__global__ void __launch_bounds__(kThreads) trid_warp_kernel(
+    int n, long long nlines, long long stride, int o1n, long long o1s, long long o2s,
+    const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
+    T *__restrict__ D, T *__restrict__ U) {
+  const int lane = threadIdx.x & 31;
+  const long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (line >= nlines) return;  // the whole warp leaves together
+  const long long base = (line % o1n) * o1s + (line / o1n) * o2s;
+  const int k0 = lane * CL;
+  const int len = max(0, min(CL, n - k0));
+  double a[CL], b[CL], c[CL], d[CL];
+#pragma unroll
+  for (int i = 0; i < CL; i++) {
+    a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
+    if (i < len) {
+      const long long e = base + (long long)(k0 + i) * stride;
+      a[i] = (k0 + i == 0) ? 0.0 : (double)A[e];      // no left neighbour
+      b[i] = (double)B[e];
+      c[i] = (k0 + i == n - 1) ? 0.0 : (double)C[e];  // no right neighbour
+      d[i] = (double)D[e];
+    }
+  }
+  chunk_reduce<CL>(a, b, c, d);
+  double xf, xl;
+  warp_pcr(a[0], c[0], d[0], a[CL - 1], c[CL - 1], d[CL - 1], lane, xf, xl);
+#pragma unroll
+  for (int i = 0; i < CL; i++)
+    if (i < len) {
+      const double x = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+      const long long e = base + (long long)(k0 + i) * stride;
+      if (INC)
+        U[e] = (T)((double)U[e] + x);
+      else
+        D[e] = (T)x;
+    }
+}
+
+// Staged warp-per-line form: the CTA's W = 8 lines pass through shared memory
+// so that loads and stores are contiguous runs.  Unit-stride lines: consecutive
+// threads take consecutive points of a line.  Strided lines: consecutive
+// threads take the same point of the 8 lines, which are neighbours along the
+// fastest other axis, so each row of the tile is one 8-element run.  Each warp
+// then solves one line from shared memory with the shuffle PCR; the solution
+// leaves through shared memory the same way.
+template <typename T, bool INC, int CL>
+__global__ void __launch_bounds__(kThreads) trid_staged_kernel(
+    int n, long long nlines, long long stride, int unit, int o1n, long long o1s, long long o2s,
+    const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
+    T *__restrict__ D, T *__restrict__ U) {
+  extern __shared__ double sm[];
+  constexpr int W = kThreads / 32;  // lines per CTA
+  constexpr int P = 32;             // chunk slots per line (lanes)
+  constexpr int pitch = CL + 1;     // padded chunk pitch (spreads the banks)
+  constexpr int per_arr = W * P * pitch;
+  double *sA = sm, *sB = sA + per_arr, *sC = sB + per_arr, *sD = sC + per_arr;
+  const int tid = threadIdx.x;
+  const long long line0 = (long long)blockIdx.x * W;
+  const int total = W * n;
+  for (int idx = tid; idx < total; idx += kThreads) {
+    int lq, k;
+    if (unit) { lq = idx / n; k = idx - lq * n; }
+    else { k = idx / W; lq = idx - k * W; }
+    const long long line = line0 + lq;
+    if (line >= nlines) continue;
+    const long long e = (line % o1n) * o1s + (line / o1n) * o2s + (long long)k * stride;
+    const int s = (lq * P + k / CL) * pitch + (k % CL);
+    sA[s] = (double)A[e];
+    sB[s] = (double)B[e];
+    sC[s] = (double)C[e];
+    sD[s] = (double)D[e];
+  }
+  __syncthreads();
+  const int w = tid >> 5, lane = tid & 31;
+  const long long line = line0 + w;
+  const int k0 = lane * CL;
+  const int len = line < nlines ? max(0, min(CL, n - k0)) : 0;
+  const int cs = (w * P + lane) * pitch;
+  double a[CL], b[CL], c[CL], d[CL];
+#pragma unroll
+  for (int i = 0; i < CL; i++) {
+    a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
+    if (i < len) {
+      a[i] = (k0 + i == 0) ? 0.0 : sA[cs + i];
+      b[i] = sB[cs + i];
+      c[i] = (k0 + i == n - 1) ? 0.0 : sC[cs + i];
+      d[i] = sD[cs + i];
+    }
+  }
+  chunk_reduce<CL>(a, b, c, d);
+  double xf, xl;
+  warp_pcr(a[0], c[0], d[0], a[CL - 1], c[CL - 1], d[CL - 1], lane, xf, xl);
+#pragma unroll
+  for (int i = 0; i < CL; i++)
+    if (i < len) sD[cs + i] = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+  __syncthreads();
+  for (int idx = tid; idx < total; idx += kThreads) {
+    int lq, k;
+    if (unit) { lq = idx / n; k = idx - lq * n; }
+    else { k = idx / W; lq = idx - k * W; }
+    const long long ln = line0 + lq;
+    if (ln >= nlines) continue;
+    const long long e = (ln % o1n) * o1s + (ln / o1n) * o2s + (long long)k * stride;
+    const double x = sD[(lq * P + k / CL) * pitch + (k % CL)];
+    if (INC)
+      U[e] = (T)((double)U[e] + x);
+    else
+      D[e] = (T)x;
+  }
+}
+
+// Long lines (n > 32*16): LPB lines per CTA, P chunks per line spread over
+// the CTA, PCR over the 2P end unknowns in shared memory.
+template <typename T, bool INC, int CL>
+__global__ void __launch_bounds__(kThreads) trid_cta_kernel(
+    int n, int P, int LPB, long long nlines, long long stride, int o1n, long long o1s,
     long long o2s, const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
     T *__restrict__ D, T *__restrict__ U) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
-  int l, p;
-  if (unit) {
-    p = tid % P;
-    l = tid / P;
-  } else {
-    l = tid % LPB;
-    p = tid / LPB;
-  }
+  const int p = tid % P, l = tid / P;
   const long long line = (long long)blockIdx.x * LPB + l;
-  const bool active = line < nlines;
+  const bool active = line < nlines && l < LPB;
   const int m = 2 * P;
-  double *ra = sm + (size_t)l * m * 3;
+  double *ra = sm + (size_t)(l < LPB ? l : 0) * m * 3;
   double *rc = ra + m;
   double *rd = rc + m;
-
   long long base = 0;
-  if (active) {
-    long long i1 = line % o1n, i2 = line / o1n;
-    base = i1 * o1s + i2 * o2s;
-  }
-  const int k0 = (int)(((long long)p * n) / P);
-  const int k1 = (int)(((long long)(p + 1) * n) / P);
-  const int len = active ? (k1 - k0) : 0;
-
-  double a[kMaxL], b[kMaxL], c[kMaxL], d[kMaxL];
+  if (active) base = (line % o1n) * o1s + (line / o1n) * o2s;
+  const int k0 = p * CL;
+  const int len = active ? max(0, min(CL, n - k0)) : 0;
+  double a[CL], b[CL], c[CL], d[CL];
 #pragma unroll
-  for (int i = 0; i < kMaxL; i++) {
+  for (int i = 0; i < CL; i++) {
     a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
     if (i < len) {
-      long long e = base + (long long)(k0 + i) * stride;
-      a[i] = (double)A[e];
+      const long long e = base + (long long)(k0 + i) * stride;
+      a[i] = (k0 + i == 0) ? 0.0 : (double)A[e];
       b[i] = (double)B[e];
-      c[i] = (double)C[e];
+      c[i] = (k0 + i == n - 1) ? 0.0 : (double)C[e];
       d[i] = (double)D[e];
     }
   }
-  if (len > 0 && k0 == 0) a[0] = 0.0;          // no left neighbour
-  if (len > 0 && k1 == n) c[len - 1] = 0.0;    // no right neighbour
-
-  chunk_reduce(len > 0 ? len : 1, a, b, c, d);
-
-  if (len >= 2) {
+  chunk_reduce<CL>(a, b, c, d);
+  if (l < LPB) {
     ra[2 * p] = a[0]; rc[2 * p] = c[0]; rd[2 * p] = d[0];
-    ra[2 * p + 1] = a[len - 1]; rc[2 * p + 1] = c[len - 1]; rd[2 * p + 1] = d[len - 1];
-  } else if (len == 1) {
-    // only when P == 1: the single row is decoupled on both sides
-    ra[0] = 0.0; rc[0] = 0.0; rd[0] = d[0];
-    ra[1] = 0.0; rc[1] = 0.0; rd[1] = d[0];
-  } else {
-    ra[2 * p] = ra[2 * p + 1] = 0.0;
-    rc[2 * p] = rc[2 * p + 1] = 0.0;
-    rd[2 * p] = rd[2 * p + 1] = 0.0;
+    ra[2 * p + 1] = a[CL - 1]; rc[2 * p + 1] = c[CL - 1]; rd[2 * p + 1] = d[CL - 1];
   }
   __syncthreads();
-
-  // parallel cyclic reduction of the 2P end unknowns of each line
   for (int s = 1; s < m; s <<= 1) {
     double na[2], nc[2], nd[2];
 #pragma unroll
@@ -158,25 +298,19 @@ __global__ void __launch_bounds__(256) trid_hybrid_kernel(
       nd[q] = (dr - k1l * d1 - k2r * d2) * inv;
     }
     __syncthreads();
-    ra[2 * p] = na[0]; rc[2 * p] = nc[0]; rd[2 * p] = nd[0];
-    ra[2 * p + 1] = na[1]; rc[2 * p + 1] = nc[1]; rd[2 * p + 1] = nd[1];
+    if (l < LPB) {
+      ra[2 * p] = na[0]; rc[2 * p] = nc[0]; rd[2 * p] = nd[0];
+      ra[2 * p + 1] = na[1]; rc[2 * p + 1] = nc[1]; rd[2 * p + 1] = nd[1];
+    }
     __syncthreads();
   }
-
   if (len <= 0) return;
-  const double xf = rd[2 * p];
-  const double xl = rd[2 * p + 1];
+  const double xf = rd[2 * p], xl = rd[2 * p + 1];
 #pragma unroll
-  for (int i = 0; i < kMaxL; i++)
+  for (int i = 0; i < CL; i++)
     if (i < len) {
-      double x;
-      if (i == 0)
-        x = xf;
-      else if (i == len - 1)
-        x = xl;
-      else
-        x = d[i] - a[i] * xf - c[i] * xl;
-      long long e = base + (long long)(k0 + i) * stride;
+      const double x = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+      const long long e = base + (long long)(k0 + i) * stride;
       if (INC)
         U[e] = (T)((double)U[e] + x);
       else
@@ -184,10 +318,87 @@ __global__ void __launch_bounds__(256) trid_hybrid_kernel(
     }
 }
 
+struct Lines {
+  int n, unit, o1n;
+  long long nlines, stride, o1s, o2s;
+};
+
+template <typename T, int CL>
+int launch_warp(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  const int warps = kThreads / 32;
+  const long long grid = (g.nlines + warps - 1) / warps;
+  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  if (u)
+    trid_warp_kernel<T, true, CL><<<(unsigned)grid, kThreads, 0, st>>>(
+        g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b, (const T *)c,
+        (T *)d, (T *)u);
+  else
+    trid_warp_kernel<T, false, CL><<<(unsigned)grid, kThreads, 0, st>>>(
+        g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b, (const T *)c,
+        (T *)d, (T *)nullptr);
+  return (int)cudaGetLastError();
+}
+
+template <typename T, int CL>
+int launch_staged(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  const int W = kThreads / 32;
+  const long long grid = (g.nlines + W - 1) / W;
+  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+  const size_t shmem = (size_t)4 * W * 32 * (CL + 1) * sizeof(double);
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  if (u) {
+    cudaFuncSetAttribute(trid_staged_kernel<T, true, CL>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    trid_staged_kernel<T, true, CL><<<(unsigned)grid, kThreads, shmem, st>>>(
+        g.n, g.nlines, g.stride, g.unit, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
+        (const T *)c, (T *)d, (T *)u);
+  } else {
+    cudaFuncSetAttribute(trid_staged_kernel<T, false, CL>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    trid_staged_kernel<T, false, CL><<<(unsigned)grid, kThreads, shmem, st>>>(
+        g.n, g.nlines, g.stride, g.unit, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
+        (const T *)c, (T *)d, (T *)nullptr);
+  }
+  return (int)cudaGetLastError();
+}
+
+template <typename T, int CL>
+int launch_cta(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  const int P = (g.n + CL - 1) / CL;
+  if (P > kThreads) return (int)cudaErrorInvalidValue;
+  const int LPB = kThreads / P;
+  const int threads = LPB * P;
+  const size_t shmem = (size_t)LPB * 2 * P * 3 * sizeof(double);
+  const long long grid = (g.nlines + LPB - 1) / LPB;
+  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  if (u)
+    trid_cta_kernel<T, true, CL><<<(unsigned)grid, threads, shmem, st>>>(
+        g.n, P, LPB, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
+        (const T *)c, (T *)d, (T *)u);
+  else
+    trid_cta_kernel<T, false, CL><<<(unsigned)grid, threads, shmem, st>>>(
+        g.n, P, LPB, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
+        (const T *)c, (T *)d, (T *)nullptr);
+  return (int)cudaGetLastError();
+}
+
+// OB2_TRID_STAGED: 0 never, 1 always, 2 strided lines only (default)
+bool use_staged(int unit) {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("OB2_TRID_STAGED");
+    v = e ? atoi(e) : 2;
+  }
+  return v == 1 || (v == 2 && !unit);
+}
+
 template <typename T>
 int launch(int ndim, int solvedim, const int *dims, const long long *strides, const void *a,
            const void *b, const void *c, void *d, void *u) {
-  const int n = dims[solvedim];
+  Lines g;
+  g.n = dims[solvedim];
   int o1 = -1, o2 = -1;
   for (int i = 0; i < 3; i++) {
     if (i == solvedim) continue;
@@ -195,29 +406,22 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   }
   const int d1 = o1 < ndim ? dims[o1] : 1;
   const int d2 = o2 < ndim ? dims[o2] : 1;
-  const long long s1 = o1 < ndim ? strides[o1] : 0;
-  const long long s2 = o2 < ndim ? strides[o2] : 0;
-  const long long nlines = (long long)d1 * d2;
-  if (n <= 0 || nlines <= 0) return 0;
-  const int P = (n + kMaxL - 1) / kMaxL;
-  if (P > kMaxThreads) return (int)cudaErrorInvalidValue;
-  const int unit = strides[solvedim] == 1 ? 1 : 0;
-  int LPB = 256 / P;
-  if (LPB < 1) LPB = 1;
-  const int threads = LPB * P;
-  const size_t shmem = (size_t)LPB * 2 * P * 3 * sizeof(double);
-  const long long grid = (nlines + LPB - 1) / LPB;
-  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
-  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
-  if (u)
-    trid_hybrid_kernel<T, true><<<(unsigned)grid, threads, shmem, st>>>(
-        n, P, LPB, nlines, unit, strides[solvedim], d1, s1, s2, (const T *)a, (const T *)b,
-        (const T *)c, (T *)d, (T *)u);
-  else
-    trid_hybrid_kernel<T, false><<<(unsigned)grid, threads, shmem, st>>>(
-        n, P, LPB, nlines, unit, strides[solvedim], d1, s1, s2, (const T *)a, (const T *)b,
-        (const T *)c, (T *)d, (T *)nullptr);
-  return (int)cudaGetLastError();
+  g.o1n = d1;
+  g.o1s = o1 < ndim ? strides[o1] : 0;
+  g.o2s = o2 < ndim ? strides[o2] : 0;
+  g.nlines = (long long)d1 * d2;
+  g.stride = strides[solvedim];
+  g.unit = g.stride == 1 ? 1 : 0;
+  if (g.n <= 0 || g.nlines <= 0) return 0;
+  if (g.n <= 32 * 16) {
+    const bool st = use_staged(g.unit);
+    if (g.n <= 32 * 4)
+      return st ? launch_staged<T, 4>(g, a, b, c, d, u) : launch_warp<T, 4>(g, a, b, c, d, u);
+    if (g.n <= 32 * 8)
+      return st ? launch_staged<T, 8>(g, a, b, c, d, u) : launch_warp<T, 8>(g, a, b, c, d, u);
+    return st ? launch_staged<T, 16>(g, a, b, c, d, u) : launch_warp<T, 16>(g, a, b, c, d, u);
+  }
+  return launch_cta<T, 16>(g, a, b, c, d, u);
 }
 
 }  // namespace

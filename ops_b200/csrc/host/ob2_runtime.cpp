@@ -285,6 +285,8 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if (r.block_x < 1) r.block_x = 32;
   if (r.block_y < 1) r.block_y = 1;
   if (r.block_z < 1) r.block_z = 1;
+  // diagnostics above 1: per-kernel device times in the timing table
+  if (r.inst.OPS_diags > 1) r.ktime = true;
   if (r.initialised) return;
   check(ob2_dev_init(r.device), "ops_init (no usable CUDA device)");
   check(ob2_dev_sm_count(&r.sms), "ops_init");
@@ -770,6 +772,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
 
   size_t red_bytes = 0;
   int nred = 0;
+  L->idx32 = 1;
   const int soa = r.inst.OPS_soa;
   for (int i = 0; i < nargs; i++) {
     ops_arg &a = args[i];
@@ -803,6 +806,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
       if (d->block->dims != block->dims && !d->e_dat) {
         // dats of other blocks are allowed as long as the dims agree
       }
+      if ((double)dat_points(d) * d->dim >= 2147483647.0) L->idx32 = 0;
       const int md = d->dim;
       const int *st = a.stencil ? a.stencil->stride : nullptr;
       long long cum = 1, off = 0;
@@ -888,13 +892,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->partials = r.partials;
   L->partials_bytes = r.partials_cap;
   L->counter = r.counter;
-  if (r.ktime) {
-    L->ev_start = kt_begin();
-  } else if (r.inst.OPS_diags > 1) {
-    ob2_event_create(&L->ev_start);
-    ob2_event_create(&L->ev_end);
-    ob2_event_record(L->ev_start);
-  }
+  L->ev_start = r.ktime ? kt_begin() : nullptr;
   return 1;
 }
 
@@ -925,15 +923,6 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
   if (r.ktime) {
     kt_end(L->ev_start, L->kernel_index);
     L->ev_start = nullptr;
-  } else if (L->ev_start) {
-    r.launches++;
-    ob2_event_record(L->ev_end);
-    float ms = 0.f;
-    check(ob2_event_elapsed_ms(L->ev_start, L->ev_end, &ms), L->name);
-    s.dev_ms += ms;
-    ob2_event_destroy(L->ev_start);
-    ob2_event_destroy(L->ev_end);
-    L->ev_start = L->ev_end = nullptr;
   } else {
     r.launches++;
   }
@@ -1028,6 +1017,7 @@ OPS_API void ops_diagnostic_output(void) {
 OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   Runtime &r = rt();
   ob2_dev_sync();
+  ktime_collect();
   std::string s;
   char line[320];
   snprintf(line, sizeof line, "\n  %-40s %8s %14s %14s %10s\n", "Timings (B200 backend)", "count",
@@ -1332,7 +1322,11 @@ static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_d
     off += s0 * strides[i];
   }
   size_t ts = a->type_size;
-  int k = kernel_slot(u ? "ops_tridMultiDimBatch_Inc" : "ops_tridMultiDimBatch");
+  static const char *names[2][3] = {
+      {"ops_tridMultiDimBatch_x", "ops_tridMultiDimBatch_y", "ops_tridMultiDimBatch_z"},
+      {"ops_tridMultiDimBatch_Inc_x", "ops_tridMultiDimBatch_Inc_y",
+       "ops_tridMultiDimBatch_Inc_z"}};
+  int k = kernel_slot(names[u ? 1 : 0][solvedim]);
   double t0 = wall();
   void *ev = kt_begin();
   int rc = ob2_trid_batch((int)ts, ndim, solvedim, dims, strides, a->data_d + off * ts,

@@ -310,6 +310,13 @@ class Translator:
         self.headers: List[str] = []
         self.header_includes: List[str] = []
         self.ndim = 0
+        # code-generation knobs (build-time environment): points per thread
+        # along y for non-reduction loops, and the minimum resident CTAs per
+        # SM given to __launch_bounds__ (caps registers per thread; default 4,
+        # measured fastest on the CloverLeaf step: more resident warps
+        # outweigh the few small register spills it causes)
+        self.py = max(1, int(os.environ.get("OPS_B200_PY", "1")))
+        self.minb = max(0, int(os.environ.get("OPS_B200_MINB", "4")))
 
     # -- discovery ---------------------------------------------------------
     def resolve_include(self, name: str, from_dir: str) -> Optional[str]:
@@ -564,15 +571,22 @@ class Translator:
         for variant, qual in (("R", "__restrict__ "), ("A", "")):
             prm = "".join(", %s *%sq%d" % (p.base_type, qual, i) for i, a, p in dats)
             prm += "".join(", %s *red%d" % (p.base_type, i) for i, a, p in reds)
+            # IDX32: element offsets in 32-bit arithmetic (every dat of the
+            # launch has fewer than 2^31 elements; decided by the runtime)
+            w("template <bool IDX32>")
             w("static __device__ __forceinline__ void %s_%s(const %s &p, int x, int y, int z%s) {" %
               (I, variant, P, prm))
             call = []
             for i, (a, p) in enumerate(zip(loop.args, kd.params)):
                 if a.kind == "dat":
                     ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
-                    w("  ACC<%s> a%d(q%d ? q%d + x * p.wx%d + y * p.wy%d + z * p.wz%d : "
-                      "(%s *)0, %s, p.ey%d, p.ez%d, p.ed%d);" %
-                      (p.base_type, i, i, i, i, i, i, p.base_type, ex, i, i, i))
+                    off = ("(IDX32 ? (long long)(x * (int)p.wx%d + y * (int)p.wy%d + z * (int)p.wz%d)"
+                           " : x * p.wx%d + y * p.wy%d + z * p.wz%d)" % (i, i, i, i, i, i))
+                    # only optional arguments can carry a null dat
+                    ptr = ("q%d ? q%d + %s : (%s *)0" % (i, i, off, p.base_type)) if a.opt \
+                        else "q%d + %s" % (i, off)
+                    w("  ACC<%s> a%d(%s, %s, p.ey%d, p.ez%d, p.ed%d);" %
+                      (p.base_type, i, ptr, ex, i, i, i))
                     call.append("a%d" % i)
                 elif a.kind == "gbl":
                     call.append("(%s *)p.g%d" % (p.base_type, i))
@@ -584,8 +598,10 @@ class Translator:
                 w("  int idx[3] = {x, y, z};")
             w("  %s(%s);" % (loop.kernel, ", ".join(call)))
             w("}")
-        w("template <bool RESTRICT>")
-        w("__global__ void __launch_bounds__(512) %s(const __grid_constant__ %s p) {" % (K, P))
+        w("template <bool RESTRICT, bool IDX32>")
+        minb = self.minb if not reds else 0
+        lb = "512, %d" % minb if minb > 0 else "512"
+        w("__global__ void __launch_bounds__(%s) %s(const __grid_constant__ %s p) {" % (lb, K, P))
         w("  const int x = p.lo0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);")
         for i, a, p in reds:
             w("  %s red%d[%s];" % (p.base_type, i, a.dim))
@@ -601,17 +617,24 @@ class Translator:
               " z += (int)(gridDim.z * blockDim.z))")
             w("      for (int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y); y < p.hi1;"
               " y += (int)(gridDim.y * blockDim.y)) {")
-            w("        if (RESTRICT) %s_R(p, x, y, z%s);" % (I, args_call))
-            w("        else %s_A(p, x, y, z%s);" % (I, args_call))
+            w("        if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
             w("      }")
             w("  }")
         else:
-            # one point per thread over the whole range
-            w("  const int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);")
+            # PY points per thread along y (consecutive rows), x / z one each
+            py = self.py
+            w("  const int y0 = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y) * %d;" % py)
             w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
-            w("  if (x < p.hi0 && y < p.hi1 && z < p.hi2) {")
-            w("    if (RESTRICT) %s_R(p, x, y, z%s);" % (I, args_call))
-            w("    else %s_A(p, x, y, z%s);" % (I, args_call))
+            w("  if (x < p.hi0 && z < p.hi2) {")
+            w("#pragma unroll")
+            w("    for (int j = 0; j < %d; j++) {" % py)
+            w("      const int y = y0 + j;")
+            w("      if (y < p.hi1) {")
+            w("        if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("      }")
+            w("    }")
             w("  }")
         if reds:
             w("  __shared__ double ob2_sh_raw[32 * 2];")
@@ -644,6 +667,8 @@ class Translator:
         w("  p.counter = L.counter;")
         w("  dim3 blk(L.block[0], L.block[1], L.block[2]);")
         w("  dim3 grd(L.grid[0], L.grid[1], L.grid[2]);")
+        if not reds and self.py > 1:
+            w("  grd.y = (L.n[1] + blk.y * %d - 1) / (blk.y * %d);" % (self.py, self.py))
         if reds:
             w("  size_t nblk = (size_t)grd.x * grd.y * grd.z;")
             w("  char *scratch = (char *)L.partials;")
@@ -665,10 +690,12 @@ class Translator:
                 w("  p.part%d = (%s *)scratch;"
                   " scratch += ((nblk * (%s) * sizeof(%s) + 255) / 256) * 256;" %
                   (i, p.base_type, a.dim, p.base_type))
-        w("  if (ob2_args_alias(args, %d))" % na)
-        w("    %s<false><<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
-        w("  else")
-        w("    %s<true><<<grd, blk, 0, (cudaStream_t)L.stream>>>(p);" % K)
+        w("  const bool al = ob2_args_alias(args, %d) != 0;" % na)
+        w("  cudaStream_t st = (cudaStream_t)L.stream;")
+        w("  if (al && L.idx32) %s<false, true><<<grd, blk, 0, st>>>(p);" % K)
+        w("  else if (al) %s<false, false><<<grd, blk, 0, st>>>(p);" % K)
+        w("  else if (L.idx32) %s<true, true><<<grd, blk, 0, st>>>(p);" % K)
+        w("  else %s<true, false><<<grd, blk, 0, st>>>(p);" % K)
         w("  ob2_loop_check_launch(&L);")
         w("  ob2_loop_end(&L);")
         w("}")
