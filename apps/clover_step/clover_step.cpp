@@ -76,6 +76,7 @@ __attribute__((visibility("default"))) double clover_step_run(int n) {
     advect_x = (advect_x == TRUE) ? FALSE : TRUE;
     clover_time = clover_time + dt;
   }
+  ops_execute();  // the loops queued after the last reduction (lazy execution)
   return clover_time;
 }
 

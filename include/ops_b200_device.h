@@ -123,6 +123,10 @@ OB2_API int ob2_trid_batch(int type_size, int ndim, int solvedim, const int *dim
 
 /* ---- loop-chain graphs: stream capture of queued work ---- */
 OB2_API int ob2_graph_begin_capture(void);
+/* Ends the capture.  *graph_exec == NULL: instantiates a new executable graph.
+ * Otherwise first tries to update *graph_exec in place with the captured
+ * launches (same topology, new kernel parameters: no instantiation); when the
+ * update is refused, replaces *graph_exec with a new instantiation. */
 OB2_API int ob2_graph_end_capture(void **graph_exec);
 OB2_API int ob2_graph_launch(void *graph_exec);
 OB2_API int ob2_graph_destroy(void *graph_exec);

@@ -58,6 +58,30 @@ typedef struct ob2_loop {
                                offsets fit 32-bit arithmetic */
 } ob2_loop;
 
+/* A generated launcher: launches one kernel variant with the parameter block
+ * `params` (which starts with int lo[3], hi[3]: the loop range) on `stream`. */
+typedef int (*ob2_launcher)(const void *params, const unsigned *grid, const unsigned *block,
+                            void *stream);
+
+/* Launch or queue one par_loop kernel.  Eager mode (OPS_B200_LAZY=0)
+ * launches now.  In lazy mode (the default) loops without reductions are
+ * queued with a copy of their parameters, halo transfers are queued with
+ * them, and the queue runs at the next flush point: a reduction loop,
+ * ops_reduction_result's loop, a constant, a solve, any call that moves data
+ * between host and device or hands out a raw pointer, ops_execute, ops_timers,
+ * or 64 queued items (OPS_B200_MAX_CHAIN).  A flushed chain is captured as a
+ * CUDA graph and replayed when the same chain recurs (OPS_B200_GRAPHS=0:
+ * plain launches).  With OPS_TILING (or OPS_B200_TILING=1) the chain runs
+ * tile by tile: skewed tiles along the slowest axis sized for the L2 budget
+ * OPS_CACHE_SIZE (MB), the GPU form of the reference's loop-chain tiling,
+ * ops_lazy.cpp:380-1187.  rows_per_thread: points each thread covers along y
+ * (the grid's y extent is derived from it per tile). */
+OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t psize,
+                        const unsigned *grid, const unsigned *block, int rows_per_thread);
+
+/* Runs everything the lazy queue holds (no-op in eager mode). */
+OPS_API void ob2_flush(void);
+
 /* Returns 0 when the range is empty (nothing to launch, ob2_loop_end not
  * needed), 1 otherwise. */
 OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int dim,

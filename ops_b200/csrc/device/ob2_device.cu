@@ -336,6 +336,17 @@ OB2_API int ob2_graph_end_capture(void **exec) {
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(g_stream, &g);
   if (e != cudaSuccess) return rc(e);
+  if (*exec) {
+    cudaGraphExecUpdateResultInfo info;
+    e = cudaGraphExecUpdate((cudaGraphExec_t)*exec, g, &info);
+    if (e == cudaSuccess) {
+      cudaGraphDestroy(g);
+      return 0;
+    }
+    (void)cudaGetLastError();  // a refused update is not an error
+    cudaGraphExecDestroy((cudaGraphExec_t)*exec);
+    *exec = nullptr;
+  }
   cudaGraphExec_t ge = nullptr;
   e = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);

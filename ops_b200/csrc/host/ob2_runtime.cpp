@@ -88,6 +88,33 @@ struct Runtime {
   struct Pending { void *a, *b; int k; };
   std::vector<Pending> pending;
   long long launches = 0;  // kernels launched by this runtime
+  // lazy loop-chain queue (see ob2_launch)
+  // lazy queue + graph replay on by default (fewer launch gaps, identical
+  // results); OPS_B200_LAZY=0 launches every loop at its call
+  bool lazy = true, tiling = false, graphs = true;
+  int tile_y = 0, tile_z = 0;  // fixed tile height (OPS_TILESIZE_Y/Z), 0 = from the cache budget
+  bool capturing = false;     // recording a loop chain into a graph
+  int max_chain = 64;         // queued items that force a flush (0: no limit)
+  double cache_mb = 40.0;   // L2 budget per tile (OPS_CACHE_SIZE, MB)
+  struct QAcc { int dat; int acc; int rmin, rmax; int flat; };  // no padding: hashed as bytes
+  struct QItem {
+    int kind;               // 0 par_loop, 1 halo group
+    ob2_launcher fn;
+    std::vector<char> prm;
+    unsigned grid[3], block[3];
+    int py, ndim, kidx;
+    int lo[3], hi[3];
+    std::vector<QAcc> acc;
+    void *tasks; int ntasks; long long max_pts;  // halo group
+  };
+  std::vector<QItem> q;
+  struct Graph {
+    void *exec = nullptr;
+    long long kernels = 0;  // kernel launches the graph replays
+    std::string params;     // parameter blocks the graph was captured with
+  };
+  std::unordered_map<std::string, Graph> graph_cache;  // key: the chain's shape
+  long long chains = 0, graph_hits = 0, graph_updates = 0, tiles_run = 0;
 };
 
 Runtime *R = nullptr;
@@ -144,6 +171,7 @@ void ensure_host(ops_dat d) {
 /* device -> host when the device copy is newer (ops_lib_core.cpp:2366-2379) */
 void get_data(ops_dat d) {
   ensure_host(d);
+  ob2_flush();
   if (d->dirty_hd == 2) {
     check(ob2_dev_d2h(d->data, d->data_d, d->mem), "ops_get_data");
     d->dirty_hd = 0;
@@ -153,6 +181,7 @@ void get_data(ops_dat d) {
 /* host -> device when the host copy is newer (ops_lib_core.cpp:2381-2392) */
 void put_data(ops_dat d) {
   if (d->dirty_hd == 1) {
+    ob2_flush();
     check(ob2_dev_h2d(d->data_d, d->data, d->mem), "ops_put_data");
     d->dirty_hd = 0;
   }
@@ -251,14 +280,289 @@ void *kt_begin() {
 }
 void kt_end(void *a, int k) {
   Runtime &r = rt();
-  r.launches++;
   if (!a) return;
   void *b = pool_event();
   ob2_event_record(b);
   r.pending.push_back({a, b, k});
 }
 
+/* ------------------------------------------------------------------------
+ * Lazy loop-chain queue.
+ *
+ * Restates the reference's lazy execution (ops_lazy.cpp:186-276,1248-1446):
+ * loops are recorded and run at the next flush point.  Two GPU-specific
+ * executions of a recorded chain:
+ *  - tiled: the chain runs tile by tile along the slowest axis, tiles sized
+ *    so that a tile's rows of every dat the chain touches fit the L2 budget,
+ *    so later loops read what earlier loops wrote from L2 instead of HBM.
+ *    Tiles are skewed per loop (the scheme of ops_construct_tile_plan,
+ *    ops_lazy.cpp:380-1187): walking the chain backwards, a loop's tile edge
+ *    is pushed past that of every later loop that depends on it through a
+ *    common dat, by that pair's stencil reach, so that each tile of a loop
+ *    finds its inputs complete and overwrites nothing a later tile still
+ *    reads.  Every point is computed by the same kernel as untiled, so the
+ *    results are identical.
+ *  - graph: the launches of a flushed chain are captured once into a CUDA
+ *    graph keyed by their parameters; a recurring identical chain replays
+ *    the graph (one launch instead of one per loop and tile).
+ * ---------------------------------------------------------------------- */
+void run_item(Runtime::QItem &it, const int *lo_t, const int *hi_t) {
+  Runtime &r = rt();
+  if (it.kind == 1) {
+    void *ev = r.capturing ? nullptr : kt_begin();
+    check(ob2_halo_run((const ob2_halo_task *)it.tasks, it.ntasks, it.max_pts),
+          "ops_halo_transfer");
+    r.launches++;
+    kt_end(ev, it.kidx);
+    return;
+  }
+  void *ev = r.capturing ? nullptr : kt_begin();
+  if (!lo_t) {
+    check(it.fn(it.prm.data(), it.grid, it.block, ob2_dev_stream()), "ops_par_loop launch");
+    r.launches++;
+    kt_end(ev, it.kidx);
+    return;
+  }
+  // re-range the launch to the tile: the parameter block starts with
+  // int lo[3], hi[3]
+  std::vector<char> p(it.prm);
+  int *lohi = (int *)p.data();
+  unsigned g[3] = {it.grid[0], it.grid[1], it.grid[2]};
+  const int td = it.ndim - 1;
+  lohi[td] = lo_t[td];
+  lohi[3 + td] = hi_t[td];
+  const unsigned rows = it.block[td] * (td == 1 ? (unsigned)it.py : 1u);
+  g[td] = (unsigned)((hi_t[td] - lo_t[td] + (int)rows - 1) / (int)rows);
+  check(it.fn(p.data(), g, it.block, ob2_dev_stream()), "ops_par_loop launch (tile)");
+  r.launches++;
+  r.tiles_run++;
+  kt_end(ev, it.kidx);
+}
+
+/* Tiled execution of queue items [b, e) (par_loops only, same dimension). */
+void run_tiled(std::vector<Runtime::QItem> &q, size_t b, size_t e) {
+  Runtime &r = rt();
+  const int nd = q[b].ndim;
+  const int td = nd - 1;
+  const size_t n = e - b;
+  // skew per loop: S[k] >= S[j] + reach for every later j depending on k
+  std::vector<long long> S(n, 0);
+  for (size_t kk = n; kk-- > 0;) {
+    Runtime::QItem &K = q[b + kk];
+    for (size_t jj = kk + 1; jj < n; jj++) {
+      Runtime::QItem &J = q[b + jj];
+      for (auto &ka : K.acc)
+        for (auto &ja : J.acc) {
+          if (ka.dat != ja.dat) continue;
+          const bool kw = ka.acc != OPS_READ, jw = ja.acc != OPS_READ;
+          long long need = 0;
+          bool dep = false;
+          if (kw) {  // J reads or writes what K wrote: J's reach above
+            dep = true;
+            need = std::max(need, (long long)std::max(0, ja.rmax));
+          }
+          if (jw) {  // J overwrites what K read: K's reach below
+            dep = true;
+            need = std::max(need, (long long)std::max(0, -ka.rmin));
+          }
+          if (dep) S[kk] = std::max(S[kk], S[jj] + need);
+        }
+    }
+  }
+  // tile height from the L2 budget: rows (planes) of every dat touched
+  long long ymin = LLONG_MAX, ymax = LLONG_MIN;
+  double row_bytes = 0.0;
+  std::vector<int> seen;
+  for (size_t k = b; k < e; k++) {
+    ymin = std::min(ymin, (long long)q[k].lo[td]);
+    ymax = std::max(ymax, (long long)q[k].hi[td]);
+    for (auto &a : q[k].acc) {
+      if (std::find(seen.begin(), seen.end(), a.dat) != seen.end()) continue;
+      seen.push_back(a.dat);
+      ops_dat d = r.dats[a.dat];
+      double rb = d->elem_size;
+      for (int i = 0; i < td; i++) rb *= d->size[i];
+      row_bytes += rb;
+    }
+  }
+  long long H = td == 2 ? r.tile_z : r.tile_y;
+  if (H <= 0) H = (long long)(r.cache_mb * 1048576.0 / std::max(1.0, row_bytes));
+  H = std::max(1LL, H);
+  const long long T = std::max(1LL, (ymax - ymin + H - 1) / H);
+  for (long long t = 0; t < T; t++) {
+    for (size_t kk = 0; kk < n; kk++) {
+      Runtime::QItem &K = q[b + kk];
+      long long lo = t == 0 ? LLONG_MIN : ymin + t * H + S[kk];
+      long long hi = t == T - 1 ? LLONG_MAX : ymin + (t + 1) * H + S[kk];
+      lo = std::max(lo, (long long)K.lo[td]);
+      hi = std::min(hi, (long long)K.hi[td]);
+      if (lo >= hi) continue;
+      int lt[3] = {K.lo[0], K.lo[1], K.lo[2]}, ht[3] = {K.hi[0], K.hi[1], K.hi[2]};
+      lt[td] = (int)lo;
+      ht[td] = (int)hi;
+      run_item(K, lt, ht);
+    }
+  }
+}
+
+bool tileable(const Runtime::QItem &it) {
+  if (it.kind != 0 || it.ndim < 2) return false;
+  for (auto &a : it.acc)
+    if (a.flat && a.acc != OPS_READ) return false;  // shared across tiles
+  return true;
+}
+
+void run_queue(std::vector<Runtime::QItem> &q) {
+  Runtime &r = rt();
+  size_t i = 0;
+  while (i < q.size()) {
+    if (r.tiling && tileable(q[i])) {
+      size_t j = i + 1;
+      while (j < q.size() && tileable(q[j]) && q[j].ndim == q[i].ndim) j++;
+      if (j - i >= 2) {
+        run_tiled(q, i, j);
+        i = j;
+        continue;
+      }
+    }
+    run_item(q[i], nullptr, nullptr);
+    i++;
+  }
+}
+
 }  // namespace
+
+/* run everything queued (no-op in eager mode) */
+OPS_API void ob2_flush(void) {
+  if (!R) return;
+  Runtime &r = rt();
+  if (r.q.empty()) return;
+  std::vector<Runtime::QItem> q;
+  q.swap(r.q);
+  r.chains++;
+  if (!r.graphs || r.ktime) {  // per-kernel event timing needs plain launches
+    run_queue(q);
+    return;
+  }
+  // shape: everything that fixes the graph's topology and launch shapes;
+  // exact: the shape plus every kernel parameter block (gbl values, dat
+  // pointers, ranges).  Same exact key: replay.  Same shape only (typically
+  // new ops_arg_gbl values such as a time step): re-capture and update the
+  // executable graph in place, which skips instantiation.
+  std::string shape, params;
+  auto put = [&shape](const void *p, size_t n) { shape.append((const char *)p, n); };
+  put(&r.tiling, sizeof r.tiling);
+  put(&r.tile_y, sizeof r.tile_y);
+  put(&r.tile_z, sizeof r.tile_z);
+  put(&r.cache_mb, sizeof r.cache_mb);
+  for (auto &it : q) {
+    put(&it.kind, sizeof it.kind);
+    put(&it.fn, sizeof it.fn);
+    const size_t np = it.prm.size();
+    put(&np, sizeof np);
+    put(it.grid, sizeof it.grid);
+    put(it.block, sizeof it.block);
+    put(&it.py, sizeof it.py);
+    put(it.lo, sizeof it.lo);
+    put(it.hi, sizeof it.hi);
+    put(&it.tasks, sizeof it.tasks);
+    put(&it.ntasks, sizeof it.ntasks);
+    put(&it.max_pts, sizeof it.max_pts);
+    for (auto &a : it.acc) put(&a, sizeof a);
+    params.append(it.prm.data(), np);
+  }
+  auto f = r.graph_cache.find(shape);
+  if (f != r.graph_cache.end() && f->second.params == params) {
+    r.graph_hits++;
+    check(ob2_graph_launch(f->second.exec), "loop-chain graph launch");
+    r.launches += f->second.kernels;
+    return;
+  }
+  if (f == r.graph_cache.end() && r.graph_cache.size() >= 256) {
+    check(ob2_dev_sync(), "graph cache");
+    for (auto &kv : r.graph_cache) ob2_graph_destroy(kv.second.exec);
+    r.graph_cache.clear();
+  }
+  Runtime::Graph &G = r.graph_cache[shape];  // exec == nullptr when new
+  if (G.exec) r.graph_updates++;
+  check(ob2_graph_begin_capture(), "loop-chain capture");
+  const long long l0 = r.launches;
+  r.capturing = true;
+  try {
+    run_queue(q);
+  } catch (...) {
+    r.capturing = false;
+    void *dummy = nullptr;
+    ob2_graph_end_capture(&dummy);
+    if (dummy) ob2_graph_destroy(dummy);
+    if (!G.exec) r.graph_cache.erase(shape);
+    throw;
+  }
+  r.capturing = false;
+  int e = ob2_graph_end_capture(&G.exec);
+  if (e) {
+    r.graph_cache.erase(shape);
+    check(e, "loop-chain capture");
+  }
+  G.kernels = r.launches - l0;
+  G.params.swap(params);
+  check(ob2_graph_launch(G.exec), "loop-chain graph launch");
+}
+
+OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t psize,
+                        const unsigned *grid, const unsigned *block, int rows_per_thread) {
+  Runtime &r = rt();
+  bool reduce = false;
+  for (int i = 0; i < L->nargs; i++)
+    if (L->red[i].acc) reduce = true;
+  if (!r.lazy || reduce) {
+    ob2_flush();
+    int e = fn(params, grid, block, L->stream);
+    if (e) {
+      OPSException ex(OPS_RUNTIME_ERROR);
+      ex << "Error: kernel launch of ops_par_loop " << L->name
+         << " failed: " << ob2_error_string(e);
+      throw ex;
+    }
+    r.launches++;
+    return;
+  }
+  Runtime::QItem it;
+  it.kind = 0;
+  it.fn = fn;
+  it.prm.assign((const char *)params, (const char *)params + psize);
+  for (int i = 0; i < 3; i++) {
+    it.grid[i] = grid[i];
+    it.block[i] = block[i];
+    it.lo[i] = L->lo[i];
+    it.hi[i] = L->hi[i];
+  }
+  it.py = rows_per_thread;
+  it.ndim = L->dim;
+  it.kidx = L->kernel_index;
+  it.tasks = nullptr;
+  it.ntasks = 0;
+  it.max_pts = 0;
+  const int td = L->dim - 1;
+  for (int i = 0; i < L->nargs; i++) {
+    ops_arg &a = L->args[i];
+    if (a.argtype != OPS_ARG_DAT || !a.opt || !a.dat) continue;
+    Runtime::QAcc qa;
+    qa.dat = a.dat->index;
+    qa.acc = a.acc;
+    qa.rmin = qa.rmax = 0;
+    qa.flat = (a.stencil && a.stencil->stride[td] == 0) ? 1 : 0;
+    if (a.stencil)
+      for (int p = 0; p < a.stencil->points; p++) {
+        const int o = td < a.stencil->dims ? a.stencil->stencil[p * a.stencil->dims + td] : 0;
+        qa.rmin = std::min(qa.rmin, o);
+        qa.rmax = std::max(qa.rmax, o);
+      }
+    it.acc.push_back(qa);
+  }
+  r.q.push_back(std::move(it));
+  if (r.max_chain > 0 && (int)r.q.size() >= r.max_chain) ob2_flush();
+}
 
 OPS_instance *OPS_instance::getOPSInstance() { return &rt().inst; }
 
@@ -278,8 +582,22 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
     if ((p = strstr(a, "OPS_BLOCK_SIZE_Y="))) r.block_y = atoi(p + 17);
     if ((p = strstr(a, "OPS_BLOCK_SIZE_Z="))) r.block_z = atoi(p + 17);
     if ((p = strstr(a, "OPS_DEVICE="))) r.device = atoi(p + 11);
+    // loop-chain tiling (ops_lib_core.cpp:132-180): lazy queue + tiles
+    if (strstr(a, "OPS_TILING")) r.lazy = r.tiling = true;
+    if ((p = strstr(a, "OPS_TILESIZE_Y="))) r.tile_y = atoi(p + 15);
+    if ((p = strstr(a, "OPS_TILESIZE_Z="))) r.tile_z = atoi(p + 15);
+    if ((p = strstr(a, "OPS_CACHE_SIZE="))) r.cache_mb = atof(p + 15);
   }
   const char *e;
+  if ((e = getenv("OPS_B200_LAZY"))) r.lazy = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_TILING"))) r.tiling = atoi(e) != 0;
+  if (r.tiling) r.lazy = true;
+  if ((e = getenv("OPS_B200_GRAPHS"))) r.graphs = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_TILESIZE_Y"))) r.tile_y = atoi(e);
+  if ((e = getenv("OPS_B200_TILESIZE_Z"))) r.tile_z = atoi(e);
+  if ((e = getenv("OPS_B200_CACHE_MB"))) r.cache_mb = atof(e);
+  if ((e = getenv("OPS_B200_MAX_CHAIN"))) r.max_chain = atoi(e);
+  if (r.cache_mb <= 0.0) r.cache_mb = 40.0;
   if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
   if ((e = getenv("OPS_B200_BLOCK"))) sscanf(e, "%d,%d,%d", &r.block_x, &r.block_y, &r.block_z);
   if (r.block_x < 1) r.block_x = 32;
@@ -299,6 +617,7 @@ OPS_API void ops_dump_dats(const char *path);
 
 OPS_API void ops_exit(void) {
   if (!R || !R->initialised) return;
+  ob2_flush();
   const char *dump = getenv("OPS_DUMP_FILE");
   if (dump && *dump) ops_dump_dats(dump);
   ob2_dev_sync();
@@ -393,6 +712,7 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
 
 OPS_API void ops_free_dat(ops_dat d) {
   if (!d) return;
+  ob2_flush();
   ob2_dev_sync();
   for (auto &p : rt().dats)
     if (p == d) p = nullptr;
@@ -403,6 +723,7 @@ OPS_API void ops_free_dat(ops_dat d) {
 
 OPS_API void ops_dat_deep_copy(ops_dat target, ops_dat src) {
   require_init();
+  ob2_flush();
   if (target->data_d && target->mem != src->mem) {
     ob2_dev_sync();
     ob2_dev_free(target->data_d);
@@ -696,18 +1017,41 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
   for (int hh = 0; !stale && hh < g->nhalos; hh++)
     stale = gx.key[2 * hh] != g->halos[hh]->from->data_d ||
             gx.key[2 * hh + 1] != g->halos[hh]->to->data_d;
-  if (stale) build_halo_tasks(g, gx);
+  if (stale) {
+    ob2_flush();  // queued transfers may still use the old task table
+    build_halo_tasks(g, gx);
+  }
   for (int hh = 0; hh < g->nhalos; hh++) {
     put_data(g->halos[hh]->from);
     put_data(g->halos[hh]->to);
   }
+  Runtime &r = rt();
   int k = kernel_slot("ops_halo_transfer");
   double t0 = wall();
-  void *ev = kt_begin();
-  check(ob2_halo_run((const ob2_halo_task *)gx.tasks_d, gx.ntasks, gx.max_pts),
-        "ops_halo_transfer");
-  kt_end(ev, k);
-  KStat &s = rt().kstats[k];
+  if (r.lazy && gx.ntasks) {
+    // part of the loop chain: ordered with the queued loops, captured with
+    // them into the chain's graph
+    Runtime::QItem it;
+    it.kind = 1;
+    it.fn = nullptr;
+    for (int i = 0; i < 3; i++) it.grid[i] = it.block[i] = 1, it.lo[i] = it.hi[i] = 0;
+    it.py = 1;
+    it.ndim = 0;
+    it.kidx = k;
+    it.tasks = gx.tasks_d;
+    it.ntasks = gx.ntasks;
+    it.max_pts = gx.max_pts;
+    r.q.push_back(std::move(it));
+    if (r.max_chain > 0 && (int)r.q.size() >= r.max_chain) ob2_flush();
+  } else {
+    ob2_flush();
+    void *ev = kt_begin();
+    check(ob2_halo_run((const ob2_halo_task *)gx.tasks_d, gx.ntasks, gx.max_pts),
+          "ops_halo_transfer");
+    kt_end(ev, k);
+    r.launches++;
+  }
+  KStat &s = r.kstats[k];
   s.count++;
   s.host_s += wall() - t0;
   for (int hh = 0; hh < g->nhalos; hh++) {
@@ -729,6 +1073,7 @@ OPS_API void ops_decl_const_char(OPS_instance *, int dim, char const *, int type
                                  char const *name) {
   require_init();
   if (!rt().const_fn) return;  // no generated kernel uses constants
+  ob2_flush();                 // queued loops read the old value
   int rc = rt().const_fn(name, dim, type_size, data, ob2_dev_stream());
   if (rc < 0) {
     OPSException ex(OPS_INVALID_ARGUMENT);
@@ -738,8 +1083,9 @@ OPS_API void ops_decl_const_char(OPS_instance *, int dim, char const *, int type
   check(rc, "ops_decl_const");
 }
 
-/* all work is stream ordered: nothing is queued host-side */
-OPS_API void ops_execute(OPS_instance *) {}
+/* runs the lazy loop-chain queue (ops_lazy.cpp:1248-1446); work is
+ * stream ordered, so this does not wait for the device */
+OPS_API void ops_execute(OPS_instance *) { ob2_flush(); }
 
 /* ------------------------------------------------------------------------
  * par_loop support for generated stubs (loop_host.cpp.j2:13-780)
@@ -797,6 +1143,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
       if (d->e_dat && (a.acc == OPS_INC || a.acc == OPS_MIN || a.acc == OPS_MAX) &&
           dx.edat_prev_acc != a.acc) {
         dx.edat_prev_acc = a.acc;
+        ob2_flush();
         unsigned char idv[8];
         int tc = type_code(d->type);
         identity_bytes(tc, a.acc, idv, true);
@@ -892,7 +1239,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->partials = r.partials;
   L->partials_bytes = r.partials_cap;
   L->counter = r.counter;
-  L->ev_start = r.ktime ? kt_begin() : nullptr;
+  L->ev_start = (r.ktime && !r.lazy) ? kt_begin() : nullptr;
   return 1;
 }
 
@@ -920,11 +1267,9 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
   Runtime &r = rt();
   KStat &s = r.kstats[L->kernel_index];
   s.count++;
-  if (r.ktime) {
+  if (L->ev_start) {
     kt_end(L->ev_start, L->kernel_index);
     L->ev_start = nullptr;
-  } else {
-    r.launches++;
   }
   s.host_s += wall() - L->host_t0;
   for (int i = 0; i < L->nargs; i++) {
@@ -945,6 +1290,7 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
  * ---------------------------------------------------------------------- */
 static void ktime_collect() {
   Runtime &r = rt();
+  ob2_flush();
   if (r.pending.empty()) return;
   check(ob2_dev_sync(), "ob2_ktime");
   for (auto &p : r.pending) {
@@ -1016,6 +1362,7 @@ OPS_API void ops_diagnostic_output(void) {
 }
 OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   Runtime &r = rt();
+  ob2_flush();
   ob2_dev_sync();
   ktime_collect();
   std::string s;
@@ -1033,6 +1380,13 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   }
   snprintf(line, sizeof line, "  Total kernel time (host): %f\n", tt);
   s += line;
+  if (r.lazy) {
+    snprintf(line, sizeof line,
+             "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "
+             "%lld tile launches\n",
+             r.chains, r.graph_hits, r.graph_updates, r.tiles_run);
+    s += line;
+  }
   if (buf && n) {
     size_t m = std::min(n - 1, s.size());
     memcpy(buf, s.data(), m);
@@ -1053,7 +1407,10 @@ OPS_API void ops_timers_core(double *cpu, double *et) {
 /* like the reference CUDA backend's ops_timers: device work is complete at
  * the returned time stamp */
 OPS_API void ops_timers(double *cpu, double *et) {
-  if (R && R->initialised) ob2_dev_sync();
+  if (R && R->initialised) {
+    ob2_flush();
+    ob2_dev_sync();
+  }
   ops_timers_core(cpu, et);
 }
 OPS_API int ops_is_root(void) { return 1; }
@@ -1158,6 +1515,7 @@ OPS_API void ops_dat_get_raw_metadata(ops_dat d, int part, int *disp, int *size,
 /* ops_dummy_singlenode.cpp:662-707 */
 OPS_API char *ops_dat_get_raw_pointer(ops_dat d, int, ops_stencil, ops_memspace *ms) {
   require_init();
+  ob2_flush();
   if (ms && *ms == OPS_HOST) {
     get_data(d);
     d->locked_hd = OPS_HOST;
@@ -1213,6 +1571,7 @@ static void slab_io(ops_dat d, char *data, const int *range, ops_memspace ms, in
   }
   size_t bytes = pts * d->elem_size;
   if (bytes == 0) return;
+  ob2_flush();
   put_data(d);
   char *buf = data;
   if (ms != OPS_DEVICE) {
@@ -1274,6 +1633,7 @@ static void fill_rand(ops_dat d, int normal) {
   if (d->type_size != 8 && d->type_size != 4)
     throw OPSException(OPS_NOT_IMPLEMENTED, "Error: random fill needs a float or double dat");
   size_t n = dat_points(d) * d->dim;
+  ob2_flush();
   check(ob2_fill_random(d->data_d, d->type_size, n, rt().rng_seed, rt().rng_counter, normal),
         "ops_fill_random");
   rt().rng_counter += n;
@@ -1328,11 +1688,13 @@ static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_d
        "ops_tridMultiDimBatch_Inc_z"}};
   int k = kernel_slot(names[u ? 1 : 0][solvedim]);
   double t0 = wall();
+  ob2_flush();
   void *ev = kt_begin();
   int rc = ob2_trid_batch((int)ts, ndim, solvedim, dims, strides, a->data_d + off * ts,
                           b->data_d + off * ts, c->data_d + off * ts, d->data_d + off * ts,
                           u ? u->data_d + off * ts : nullptr);
   kt_end(ev, k);
+  rt().launches++;
   if (rc) {
     OPSException ex(OPS_RUNTIME_ERROR);
     ex << "Tridsolver error: " << ob2_error_string(rc) << " (line length "

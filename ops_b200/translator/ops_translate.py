@@ -649,6 +649,16 @@ class Translator:
             w("    ob2::reset_counter(p.counter);")
             w("  }")
         w("}")
+        # launchers: the runtime launches a loop now or, in lazy mode, later
+        # (possibly once per tile, possibly inside a graph capture)
+        LN = "ob2l_" + loop.stub[len("ops_par_loop_"):]
+        for rs, ix in (("false", "false"), ("false", "true"), ("true", "false"), ("true", "true")):
+            w("static int %s_%s_%s(const void *prm, const unsigned *g, const unsigned *b,"
+              " void *st) {" % (LN, rs[0], ix[0]))
+            w("  %s<%s, %s><<<dim3(g[0], g[1], g[2]), dim3(b[0], b[1], b[2]), 0,"
+              " (cudaStream_t)st>>>(*(const %s *)prm);" % (K, rs, ix, P))
+            w("  return (int)cudaGetLastError();")
+            w("}")
         # host stub
         params = ", ".join("ops_arg arg%d" % i for i in range(len(loop.args)))
         ns = re.sub(r"\W", "_", self.app)
@@ -691,12 +701,10 @@ class Translator:
                   " scratch += ((nblk * (%s) * sizeof(%s) + 255) / 256) * 256;" %
                   (i, p.base_type, a.dim, p.base_type))
         w("  const bool al = ob2_args_alias(args, %d) != 0;" % na)
-        w("  cudaStream_t st = (cudaStream_t)L.stream;")
-        w("  if (al && L.idx32) %s<false, true><<<grd, blk, 0, st>>>(p);" % K)
-        w("  else if (al) %s<false, false><<<grd, blk, 0, st>>>(p);" % K)
-        w("  else if (L.idx32) %s<true, true><<<grd, blk, 0, st>>>(p);" % K)
-        w("  else %s<true, false><<<grd, blk, 0, st>>>(p);" % K)
-        w("  ob2_loop_check_launch(&L);")
+        w("  const ob2_launcher fn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
+          " : (L.idx32 ? %s_t_t : %s_t_f);" % (LN, LN, LN, LN))
+        w("  const unsigned g3[3] = {grd.x, grd.y, grd.z}, b3[3] = {blk.x, blk.y, blk.z};")
+        w("  ob2_launch(&L, fn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else self.py))
         w("  ob2_loop_end(&L);")
         w("}")
         w("namespace ob2_%s {" % ns)

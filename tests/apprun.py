@@ -28,10 +28,11 @@ def ensure(name: str, flavour: str, shared: bool = True) -> str:
     return catalog.build(name, flavour, shared=shared)
 
 
-def run_app(name: str, flavour: str, args=(), dump: bool = False, cwd=None, timeout=900):
-    """Returns (stdout, dump_path or None)."""
+def run_app(name: str, flavour: str, args=(), dump: bool = False, cwd=None, timeout=900,
+            env=None):
+    """Returns (stdout, dump_path or None).  env: extra environment variables."""
     ensure(name, flavour, shared=True)
-    env = dict(os.environ)
+    env = dict(os.environ, **(env or {}))
     dpath = None
     if dump:
         fd, dpath = tempfile.mkstemp(prefix="%s_%s_" % (name, flavour), suffix=".dump")

@@ -1,0 +1,81 @@
+"""GPU tests of lazy execution: the loop-chain queue, its tiled execution and
+its CUDA-graph replay give results bit-identical to eager execution.
+
+Tiled execution runs every point through the same kernel as eager execution,
+only split into skewed row tiles, so every dat must match exactly (max
+difference 0).  Small forced tile heights (OPS_B200_TILESIZE_Y/Z) make many
+tiles per chain, so the skew of every dependency pair is exercised.
+"""
+
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from tests.apprun import ROOT, ensure, result_lines, run_app
+from tests.opsdump import compare
+
+pytestmark = pytest.mark.gpu
+
+EAGER = {"OPS_B200_LAZY": "0", "OPS_B200_TILING": "0"}
+MODES = {
+    "lazy_graphs": {"OPS_B200_LAZY": "1", "OPS_B200_TILING": "0", "OPS_B200_GRAPHS": "1"},
+    "tiled_plain": {"OPS_B200_TILING": "1", "OPS_B200_GRAPHS": "0", "OPS_B200_TILESIZE_Y": "7",
+                    "OPS_B200_TILESIZE_Z": "3"},
+    "tiled_graphs": {"OPS_B200_TILING": "1", "OPS_B200_GRAPHS": "1", "OPS_B200_TILESIZE_Y": "5",
+                     "OPS_B200_TILESIZE_Z": "2"},
+    "tiled_cache": {"OPS_B200_TILING": "1", "OPS_B200_GRAPHS": "1", "OPS_B200_CACHE_MB": "0.25"},
+}
+
+
+def numbers_only(lines):
+    """result lines without their timing fields"""
+    return [re.sub(r"\S+ ms/step|\S+ s\b|\S+ GLUPS", "", l) for l in lines]
+
+
+def same(a, b):
+    d = compare(a, b)
+    bad = {k: v for k, v in d.items() if v != 0.0}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
+@pytest.mark.parametrize("app,args", [
+    ("poisson_mb", ["-nb=1", "-n=200", "-sweeps=40", "-check=10"]),
+    ("poisson_mb", ["-nb=3", "-n=61", "-sweeps=25", "-check=5"]),
+    ("opsunit", ["-nx=45", "-ny=38"]),
+    ("adi3d", ["-nx=40", "-ny=23", "-nz=17", "-steps=3", "-prec=64"]),
+])
+def test_lazy_matches_eager(app, args, mode):
+    eo, ed = run_app(app, "b200", args, dump=True, env=EAGER)
+    lo, ld = run_app(app, "b200", args, dump=True, env=MODES[mode])
+    same(ld, ed)
+    assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
+
+
+@pytest.mark.parametrize("mode", ["lazy_graphs", "tiled_graphs", "tiled_cache"])
+def test_cloverleaf_lazy_matches_eager(tmp_path, mode):
+    ensure("clover_step", "b200")
+    dumps = {}
+    for tag, env in (("eager", EAGER), (mode, MODES[mode])):
+        dumps[tag] = str(tmp_path / ("%s.dump" % tag))
+        r = subprocess.run([sys.executable, "-m", "apps.clover_run", "--flavour", "b200",
+                            "--cells", "120", "--steps", "12", "--dump", dumps[tag]], cwd=ROOT,
+                           env=dict(os.environ, **env), capture_output=True, text=True,
+                           timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+    same(dumps[mode], dumps["eager"])
+
+
+def test_mblock_halos_lazy_matches_eager(tmp_path):
+    """Queued ops_halo_transfer groups (multi-block, permuted and flipped)."""
+    exe = ensure("ref_mblock", "b200", shared=False)
+    dumps = {}
+    for tag, env in (("eager", EAGER), ("lazy", MODES["tiled_graphs"])):
+        dumps[tag] = str(tmp_path / ("%s.dump" % tag))
+        r = subprocess.run([exe], cwd=str(tmp_path), capture_output=True, text=True,
+                           env=dict(os.environ, OPS_DUMP_FILE=dumps[tag], **env), timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+    same(dumps["lazy"], dumps["eager"])
