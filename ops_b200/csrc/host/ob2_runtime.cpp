@@ -95,6 +95,7 @@ struct Runtime {
   int tile_y = 0, tile_z = 0;  // fixed tile height (OPS_TILESIZE_Y/Z), 0 = from the cache budget
   bool capturing = false;     // recording a loop chain into a graph
   int max_chain = 64;         // queued items that force a flush (0: no limit)
+  int red_waves = 1;          // reduction grids: waves of resident CTAs (OPS_B200_RED_WAVES)
   double cache_mb = 40.0;   // L2 budget per tile (OPS_CACHE_SIZE, MB)
   struct QAcc { int dat; int acc; int rmin, rmax; int flat; };  // no padding: hashed as bytes
   struct QItem {
@@ -517,7 +518,9 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t
     if (L->red[i].acc) reduce = true;
   if (!r.lazy || reduce) {
     ob2_flush();
+    void *ev = kt_begin();
     int e = fn(params, grid, block, L->stream);
+    kt_end(ev, L->kernel_index);
     if (e) {
       OPSException ex(OPS_RUNTIME_ERROR);
       ex << "Error: kernel launch of ops_par_loop " << L->name
@@ -597,6 +600,7 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_TILESIZE_Z"))) r.tile_z = atoi(e);
   if ((e = getenv("OPS_B200_CACHE_MB"))) r.cache_mb = atof(e);
   if ((e = getenv("OPS_B200_MAX_CHAIN"))) r.max_chain = atoi(e);
+  if ((e = getenv("OPS_B200_RED_WAVES"))) r.red_waves = std::max(1, atoi(e));
   if (r.cache_mb <= 0.0) r.cache_mb = 40.0;
   if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
   if ((e = getenv("OPS_B200_BLOCK"))) sscanf(e, "%d,%d,%d", &r.block_x, &r.block_y, &r.block_z);
@@ -1206,7 +1210,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   {
     long long tpb = (long long)L->block[0] * L->block[1] * L->block[2];
     long long per_sm = std::max(1LL, 2048 / tpb);
-    long long target = (long long)r.sms * per_sm;
+    long long target = (long long)r.sms * per_sm * r.red_waves;
     long long gx = (L->n[0] + L->block[0] - 1) / L->block[0];
     long long gy = (L->n[1] + L->block[1] - 1) / L->block[1];
     long long gz = (L->n[2] + L->block[2] - 1) / L->block[2];
@@ -1239,7 +1243,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->partials = r.partials;
   L->partials_bytes = r.partials_cap;
   L->counter = r.counter;
-  L->ev_start = (r.ktime && !r.lazy) ? kt_begin() : nullptr;
+  L->ev_start = nullptr;  // launches are timed in ob2_launch / run_item
   return 1;
 }
 

@@ -315,7 +315,11 @@ class Translator:
         # SM given to __launch_bounds__ (caps registers per thread; default 4,
         # measured fastest on the CloverLeaf step: more resident warps
         # outweigh the few small register spills it causes)
+        self.py_forced = "OPS_B200_PY" in os.environ
         self.py = max(1, int(os.environ.get("OPS_B200_PY", "1")))
+        # strided rows per trip of a reduction kernel's row loop (at least)
+        self.rpy = max(1, int(os.environ.get("OPS_B200_RPY", "1")))
+        self.light_max = int(os.environ.get("OPS_B200_LIGHT", "4"))
         self.minb = max(0, int(os.environ.get("OPS_B200_MINB", "4")))
 
     # -- discovery ---------------------------------------------------------
@@ -489,6 +493,7 @@ class Translator:
         w('#include "ops_b200_loop.h"')
         w('#include "ops_b200_kernel.h"')
         w("#include <cuda_runtime.h>")
+        w("#include <algorithm>")
         # user headers that kernel headers depend on (types, macros)
         for h in self.cu_includes():
             w('#include "%s"' % h)
@@ -536,6 +541,33 @@ class Translator:
         w("}  // namespace")
         with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
             f.write("\n".join(L) + "\n")
+
+    ELEM_BYTES = {"double": 8, "long long": 8, "int64_t": 8, "unsigned long long": 8,
+                  "float": 4, "int": 4, "unsigned int": 4, "unsigned": 4, "int32_t": 4,
+                  "short": 2, "half": 2, "__half": 2, "char": 1, "unsigned char": 1,
+                  "bool": 1}
+
+    def light_y_stencil(self, kd) -> bool:
+        """True for a short kernel body (OPS_B200_LIGHT statements at most,
+        default 4) that reads a
+        neighbour along y, e.g. u(0, 1): consecutive rows handled by one
+        thread then share those loads in registers."""
+        body = kd.text[kd.text.find("{"):]
+        if mask_comments_strings(body).count(";") > self.light_max:
+            return False
+        return re.search(r"\w\s*\(\s*(?:\d+\s*,\s*)?-?\d+\s*,\s*-?[1-9]\d*\s*[,)]",
+                         body) is not None
+
+    def rows_per_thread(self, dats, kd=None) -> int:
+        """Points per thread along y.  OPS_B200_PY when set; otherwise 2 for
+        a light kernel with a y stencil (register reuse of the shared rows)
+        and 1 for the rest.  Loops whose widest dat element is narrower than
+        8 bytes take proportionally more rows, so each thread keeps the same
+        bytes in flight."""
+        base = self.py if self.py_forced else (2 if kd is not None and
+                                               self.light_y_stencil(kd) else 1)
+        widest = max([self.ELEM_BYTES.get(p.base_type, 8) for i, a, p in dats] or [8])
+        return base * max(1, 8 // widest)
 
     def emit_loop(self, loop: Loop, w) -> None:
         kd = self.kernels[loop.kernel]
@@ -609,32 +641,62 @@ class Translator:
               (a.dim, i, p.base_type, a.acc))
         args_call = "".join(", p.b%d" % i for i, a, p in dats) + \
             "".join(", red%d" % i for i, a, p in reds)
+        py = self.rows_per_thread(dats, kd)
         if reds:
+            py = max(py, self.rpy)
             # reductions: grid of about one wave of resident CTAs, threads
-            # stride over y and z, so that few per-CTA partials are combined
+            # stride over y and z, so that few per-CTA partials are combined;
+            # PY strided rows per trip, so that their loads are in flight
+            # together
             w("  if (x < p.hi0) {")
+            w("    const int ys = (int)(gridDim.y * blockDim.y) * %d;" % py)
             w("    for (int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z); z < p.hi2;"
               " z += (int)(gridDim.z * blockDim.z))")
-            w("      for (int y = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y); y < p.hi1;"
-              " y += (int)(gridDim.y * blockDim.y)) {")
-            w("        if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
-            w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("      for (int yb = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y) * %d;"
+              " yb < p.hi1; yb += ys) {" % py)
+            # PY consecutive rows per trip; all in range: no branch between
+            # the calls, so the loads of every row can be issued before the
+            # stores of the first, and rows shared by the stencils are loaded
+            # once
+            w("        if (yb + %d < p.hi1) {" % (py - 1))
+            w("#pragma unroll")
+            w("          for (int j = 0; j < %d; j++) {" % py)
+            w("            if (RESTRICT) %s_R<IDX32>(p, x, yb + j, z%s);" % (I, args_call))
+            w("            else %s_A<IDX32>(p, x, yb + j, z%s);" % (I, args_call))
+            w("          }")
+            w("        } else {")
+            w("          for (int y = yb; y < p.hi1; y++) {")
+            w("            if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("            else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("          }")
+            w("        }")
             w("      }")
             w("  }")
         else:
             # PY points per thread along y (consecutive rows), x / z one each
-            py = self.py
             w("  const int y0 = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y) * %d;" % py)
             w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
             w("  if (x < p.hi0 && z < p.hi2) {")
-            w("#pragma unroll")
-            w("    for (int j = 0; j < %d; j++) {" % py)
-            w("      const int y = y0 + j;")
-            w("      if (y < p.hi1) {")
-            w("        if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
-            w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
-            w("      }")
-            w("    }")
+            if py == 1:
+                w("    if (y0 < p.hi1) {")
+                w("      if (RESTRICT) %s_R<IDX32>(p, x, y0, z%s);" % (I, args_call))
+                w("      else %s_A<IDX32>(p, x, y0, z%s);" % (I, args_call))
+                w("    }")
+            else:
+                # all PY rows in range: no branch between the calls (loads of
+                # every row may be issued before the first row's stores)
+                w("    if (y0 + %d < p.hi1) {" % (py - 1))
+                w("#pragma unroll")
+                w("      for (int j = 0; j < %d; j++) {" % py)
+                w("        if (RESTRICT) %s_R<IDX32>(p, x, y0 + j, z%s);" % (I, args_call))
+                w("        else %s_A<IDX32>(p, x, y0 + j, z%s);" % (I, args_call))
+                w("      }")
+                w("    } else {")
+                w("      for (int y = y0; y < p.hi1; y++) {")
+                w("        if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
+                w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
+                w("      }")
+                w("    }")
             w("  }")
         if reds:
             w("  __shared__ double ob2_sh_raw[32 * 2];")
@@ -644,8 +706,8 @@ class Translator:
                   (p.base_type, a.acc, i, a.dim, i, p.base_type))
             w("  if (ob2::last_block(p.counter, &ob2_flag)) {")
             for i, a, p in reds:
-                w("    ob2::final_combine<%s, %s>(%s, p.part%d, p.r%d, p.first%d, (%s *)ob2_sh_raw);" %
-                  (p.base_type, a.acc, a.dim, i, i, i, p.base_type))
+                w("    ob2::final_combine<%s, %s>(%s, p.part%d, p.r%d, p.first%d,"
+                  " (%s *)ob2_sh_raw);" % (p.base_type, a.acc, a.dim, i, i, i, p.base_type))
             w("    ob2::reset_counter(p.counter);")
             w("  }")
         w("}")
@@ -677,8 +739,11 @@ class Translator:
         w("  p.counter = L.counter;")
         w("  dim3 blk(L.block[0], L.block[1], L.block[2]);")
         w("  dim3 grd(L.grid[0], L.grid[1], L.grid[2]);")
-        if not reds and self.py > 1:
-            w("  grd.y = (L.n[1] + blk.y * %d - 1) / (blk.y * %d);" % (self.py, self.py))
+        if not reds and py > 1:
+            w("  grd.y = (L.n[1] + blk.y * %d - 1) / (blk.y * %d);" % (py, py))
+        elif reds and py > 1:
+            w("  grd.y = std::max(1u, std::min(grd.y, (unsigned)((L.n[1] + blk.y * %d - 1) /"
+              " (blk.y * %d))));" % (py, py))
         if reds:
             w("  size_t nblk = (size_t)grd.x * grd.y * grd.z;")
             w("  char *scratch = (char *)L.partials;")
@@ -704,7 +769,7 @@ class Translator:
         w("  const ob2_launcher fn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
           " : (L.idx32 ? %s_t_t : %s_t_f);" % (LN, LN, LN, LN))
         w("  const unsigned g3[3] = {grd.x, grd.y, grd.z}, b3[3] = {blk.x, blk.y, blk.z};")
-        w("  ob2_launch(&L, fn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else self.py))
+        w("  ob2_launch(&L, fn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")
         w("}")
         w("namespace ob2_%s {" % ns)

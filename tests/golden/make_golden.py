@@ -11,7 +11,8 @@ Contents
     they come from (Poisson defaults, CloverLeaf test problems 1 and 2,
     Laplace step7);
   * the printed results of this repository's drivers (multi-block Poisson,
-    opsunit) when built on the reference's sequential backend (ref_seq).
+    opsunit, CG heat conduction) when built on the reference's sequential
+    backend (ref_seq).
 """
 
 from __future__ import annotations
@@ -67,13 +68,16 @@ def main():
         "poisson_mb_3x3": ("poisson_mb", ["-nb=3", "-n=40", "-sweeps=300", "-check=50"]),
         "opsunit_default": ("opsunit", []),
         "opsunit_29x17": ("opsunit", ["-nx=29", "-ny=17"]),
+        "heat_cg_128": ("heat_cg", ["-n=128"]),
+        "heat_cg_96_fixed": ("heat_cg", ["-n=96", "-dt=2e-4", "-tol=0", "-maxit=40"]),
     }
     for key, (name, args) in cases.items():
         exe = catalog.build(name, "ref_seq")
         out = run(exe, args)
         lines = [l for l in out.splitlines()
                  if l.split() and l.split()[0] in ("sweep", "checksum", "sums", "min", "max",
-                                                   "count", "fetch_b")]
+                                                   "count", "fetch_b", "fp64", "mixed",
+                                                   "compare")]
         g["reference_runs"][key] = {"app": name, "args": args, "backend": "reference ref_seq",
                                     "lines": lines}
     with open(os.path.join(HERE, "golden.json"), "w") as f:

@@ -130,3 +130,45 @@ def test_reference_mblock_halos_match_oracle(tmp_path):
         assert r.returncode == 0, r.stderr[-2000:]
     diffs = compare(dumps["b200"], dumps["oracle"])
     assert max(diffs.values()) == 0.0, diffs
+
+
+HEAT_KEYS = ("fp64", "mixed", "compare")
+
+
+def words_and_counts(line):
+    """the line's words and integer fields (iteration counts), without the
+    floating-point values"""
+    return [t for t in line.split() if not re.search(r"[.eE]\d|\d[.eE]", t)]
+
+
+def test_heat_cg_fixed_iterations_match_oracle(golden):
+    """40 CG iterations without a stopping test, FP64 and mixed: the dats
+    against the oracle's.  The dot products are summed in a different order
+    (tree vs sequential), so alpha and beta differ in the last bits and the
+    iterates drift apart at round-off: FP64 dats within 1e-10 of the field's
+    scale; FP32 dats within 1e-5 of the field's scale (an FP32 alpha that
+    rounds the other way moves every point by one float ulp)."""
+    g = golden["reference_runs"]["heat_cg_96_fixed"]
+    gout, gd = run_app("heat_cg", "b200", g["args"], dump=True)
+    cout, cd = run_app("heat_cg", "oracle", g["args"], dump=True)
+    check_dumps(gd, cd, tol=1e-10, float_tol=1e-5, floor_frac=1.0)
+    got, want = result_lines(gout, HEAT_KEYS), g["lines"]
+    assert [words_and_counts(l) for l in got] == [words_and_counts(l) for l in want]
+    assert_lines_close(got[:2], want[:2], 1e-9)
+
+
+def test_heat_cg_converged_matches_reference(golden):
+    """Both solvers to 1e-10 relative residual on 128^2: same iteration and
+    refinement counts as the reference's sequential backend, checksums of the
+    solutions within 1e-11."""
+    g = golden["reference_runs"]["heat_cg_128"]
+    gout, _ = run_app("heat_cg", "b200", g["args"])
+    got = result_lines(gout, HEAT_KEYS)
+    want = g["lines"]
+    assert [words_and_counts(l) for l in got] == [words_and_counts(l) for l in want]
+    for key in ("fp64 checksum", "mixed checksum"):
+        a = [l for l in got if l.startswith(key)]
+        b = [l for l in want if l.startswith(key)]
+        assert_lines_close(a, b, 1e-11)
+    rel = [float(l.split()[-1]) for l in got if l.startswith("fp64 it")][0]
+    assert rel <= 1e-10

@@ -55,3 +55,16 @@ def test_reference_cloverleaf_test1_on_oracle(golden):
     assert "This test is considered PASSED" in out
     m = re.search(r"within (\S+) %", out)
     assert float(m.group(1)) < 1e-9
+
+
+HEAT_KEYS = ("fp64", "mixed", "compare")
+
+
+@pytest.mark.parametrize("case", ["heat_cg_128", "heat_cg_96_fixed"])
+def test_heat_cg_oracle_matches_reference(golden, case):
+    """CG heat conduction (FP64 CG and FP32-inner / FP64-refinement): the
+    oracle's iteration counts, residuals and checksums against the same
+    driver on the reference's sequential backend."""
+    g = golden["reference_runs"][case]
+    out, _ = run_app("heat_cg", "oracle", g["args"])
+    assert_lines_close(result_lines(out, HEAT_KEYS), g["lines"], 1e-11)
