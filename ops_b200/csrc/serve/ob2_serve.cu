@@ -22,6 +22,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "ops_b200_serve.h"
@@ -109,6 +110,12 @@ __device__ __forceinline__ double hash_uniform(int seed, int i, int j, int k) {
 constexpr int CTA_Y = 8;
 constexpr int NPART = 2;  // partial sums per tile: (p', w) and (r, r)
 
+// resident CTAs per SM the Poisson kernels are compiled for (register cap)
+#ifndef OB2S_MINB
+#define OB2S_MINB 4
+#endif
+#define POIS_BOUNDS __launch_bounds__(256, OB2S_MINB)
+
 // fixed-order CTA sum of NV values per thread; result in thread 0
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[32]) {
@@ -134,7 +141,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[32]) {
 
 // p' = r + beta p and w = A p' over the tile, (p', w) per tile (phase 2)
 template <typename TI, int RY>
-__global__ void __launch_bounds__(TX *CTA_Y) pois_pw(const Work *__restrict__ W, Req *R) {
+__global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
   __shared__ double sh[1][32];
   const long long total = W->pois_pref[W->npois];
   for (long long un = blockIdx.x; un < total; un += gridDim.x) {
@@ -155,10 +162,10 @@ __global__ void __launch_bounds__(TX *CTA_Y) pois_pw(const Work *__restrict__ W,
       // rows j0-1 .. j0+RY of column i (storage rows clamped into the
       // array; the halo rows and columns of r and p hold zeros)
       TI pc[RY + 2], pwv[RY], pev[RY];
-      long long o[RY + 2];
+      int o[RY + 2];  // (n + 2)^2 < 2^31 for n <= 32768
 #pragma unroll
       for (int m = 0; m < RY + 2; m++) {
-        o[m] = (long long)(min(j0 + m - 1, n) + 1) * P + (i + 1);
+        o[m] = (min(j0 + m - 1, n) + 1) * P + (i + 1);
         pc[m] = rr[o[m]] + beta * pin[o[m]];
       }
 #pragma unroll
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(TX *CTA_Y) pois_pw(const Work *__restrict__ W,
 // phase 2: x += alpha p', r -= alpha w, (r, r); phases 0, 3: r = b - A x in
 // FP64 and its (r, r)
 template <typename TI, int RY>
-__global__ void __launch_bounds__(TX *CTA_Y) pois_xr(const Work *__restrict__ W, Req *R) {
+__global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
   __shared__ double sh[1][32];
   const long long total = W->pois_pref[W->npois];
   for (long long un = blockIdx.x; un < total; un += gridDim.x) {
@@ -198,9 +205,9 @@ __global__ void __launch_bounds__(TX *CTA_Y) pois_xr(const Work *__restrict__ W,
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
     double v[1] = {0.0};
     if (i < n && j0 < n) {
-      long long o[RY];
+      int o[RY];  // (n + 2)^2 < 2^31 for n <= 32768
 #pragma unroll
-      for (int m = 0; m < RY; m++) o[m] = (long long)(min(j0 + m, n - 1) + 1) * P + (i + 1);
+      for (int m = 0; m < RY; m++) o[m] = (min(j0 + m, n - 1) + 1) * P + (i + 1);
       TI *rr = (TI *)q.r;
       double *x = q.x;
       if (ph == 2) {
@@ -468,6 +475,7 @@ struct ob2s_engine {
   std::vector<void *> mem;  // per slot allocation
   std::vector<size_t> bytes;
   bool work_dirty;
+  int pois_ctas_per_sm;  // resident CTAs per SM of the Poisson kernels
   struct Graph {
     int iters, variant, kernels;
     cudaGraphExec_t exec;
@@ -495,7 +503,7 @@ template <typename TI, int RY>
 static int launch_iteration(ob2s_engine *e, int variant) {
   int k = 0;
   if (variant & 1) {
-    const int g = e->sms * (2048 / (TX * CTA_Y));
+    const int g = e->sms * e->pois_ctas_per_sm;
     pois_pw<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
     scalars_a<<<MAXA, 256, 0, e->st>>>(e->W_d, e->R_d);
     pois_xr<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
@@ -550,6 +558,30 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
           cudaSuccess) {
     delete e;
     return rc(err);
+  }
+  {
+    // persistent grids: as many CTAs as can be resident at once
+    int nb = 0, nb2 = 0;
+    const bool mixed = mode == OB2S_MIXED;
+    auto occ = [&](const void *f) {
+      int b = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, TX * CTA_Y, 0);
+      return b;
+    };
+    switch (tile_y) {
+      case 8:
+        nb = occ(mixed ? (const void *)pois_pw<float, 1> : (const void *)pois_pw<double, 1>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 1> : (const void *)pois_xr<double, 1>);
+        break;
+      case 16:
+        nb = occ(mixed ? (const void *)pois_pw<float, 2> : (const void *)pois_pw<double, 2>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 2> : (const void *)pois_xr<double, 2>);
+        break;
+      default:
+        nb = occ(mixed ? (const void *)pois_pw<float, 4> : (const void *)pois_pw<double, 4>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 4> : (const void *)pois_xr<double, 4>);
+    }
+    e->pois_ctas_per_sm = std::max(1, std::min(nb, nb2));
   }
   e->R.assign(MAXA, Req());
   memset(e->R.data(), 0, sizeof(Req) * MAXA);
