@@ -153,31 +153,36 @@ __global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
     const int i = (t % q.tiles_x) * TX + threadIdx.x;
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
     double v[1] = {0.0};
-    if (i < n && j0 < n) {
+    if (j0 < n) {  // uniform over the warp (one threadIdx.y per warp)
       const TI *rr = (const TI *)q.r;
       const TI *pin = (const TI *)(q.par ? q.p1 : q.p0);
       TI *pout = (TI *)(q.par ? q.p0 : q.p1);
       TI *ww = (TI *)q.w;
       const TI beta = (TI)q.beta;
-      // rows j0-1 .. j0+RY of column i (storage rows clamped into the
-      // array; the halo rows and columns of r and p hold zeros)
-      TI pc[RY + 2], pwv[RY], pev[RY];
+      const bool inx = i < n;
+      const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
+      const int lane = threadIdx.x;
+      // p' = r + beta p on rows j0-1 .. j0+RY of column i (storage rows
+      // clamped into the array; the halo rows and columns of r and p hold
+      // zeros); a lane past the right edge stands for the zero halo column
+      TI pc[RY + 2];
       int o[RY + 2];  // (n + 2)^2 < 2^31 for n <= 32768
 #pragma unroll
       for (int m = 0; m < RY + 2; m++) {
-        o[m] = (min(j0 + m - 1, n) + 1) * P + (i + 1);
-        pc[m] = rr[o[m]] + beta * pin[o[m]];
+        o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
+        pc[m] = inx ? rr[o[m]] + beta * pin[o[m]] : (TI)0;
       }
 #pragma unroll
       for (int m = 0; m < RY; m++) {
-        pwv[m] = rr[o[m + 1] - 1] + beta * pin[o[m + 1] - 1];
-        pev[m] = rr[o[m + 1] + 1] + beta * pin[o[m + 1] + 1];
-      }
-#pragma unroll
-      for (int m = 0; m < RY; m++) {
-        if (j0 + m >= n) continue;
+        // west / east neighbours from the adjacent lanes; the warp's edge
+        // lanes form theirs from memory (the same arithmetic, same bits)
+        TI pw = __shfl_up_sync(0xffffffffu, pc[m + 1], 1);
+        TI pe = __shfl_down_sync(0xffffffffu, pc[m + 1], 1);
+        if (lane == 0) pw = rr[o[m + 1] - 1] + beta * pin[o[m + 1] - 1];
+        if (lane == TX - 1 && inx) pe = rr[o[m + 1] + 1] + beta * pin[o[m + 1] + 1];
+        if (!inx || j0 + m >= n) continue;
         const TI c = pc[m + 1];
-        const TI a = (TI)4 * c - pwv[m] - pev[m] - pc[m] - pc[m + 2];
+        const TI a = (TI)4 * c - pw - pe - pc[m] - pc[m + 2];
         pout[o[m + 1]] = c;
         ww[o[m + 1]] = a;
         v[0] += (double)c * (double)a;
