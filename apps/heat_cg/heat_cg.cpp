@@ -8,13 +8,16 @@
  * Two solvers on the same system:
  *   fp64   plain FP64 CG (TeaLeaf's unpreconditioned CG, tea_leaf_cg.cpp) to a
  *          relative residual tol;
- *   mixed  FP64 iterative refinement: r = b - A x in FP64, then FP32 CG on
- *          A d = r (FP32 dats and arithmetic, dot products accumulated in
- *          FP64) to a relative inner tolerance, x += d in FP64; repeated
- *          until the FP64 residual is below tol relative to the first one.
+ *   mixed  CG with r, w, p stored and computed in FP32 (dot products
+ *          accumulated in FP64) and the iterate x in FP64; the residual is
+ *          replaced by b - A x computed in FP64 whenever it has dropped by
+ *          the factor -inner= since the last such evaluation (iterative
+ *          refinement that keeps the search direction), and convergence is
+ *          tested on that FP64 residual.
  *
  * Options: -n= (cells per side, default 4096) -prec=64|32|both (default both)
- *          -tol= (default 1e-10) -inner= (inner relative tolerance, 1e-4)
+ *          -tol= (default 1e-10) -inner= (residual drop between FP64
+ *          residual replacements, default 1e-2)
  *          -maxit= (iteration cap per CG, default 20000) -dt= (default 4e-6)
  *          -seed= (circle centre, default 4) -useed= (u0, default 5)
  * Prints per solver: iterations, recursive and true relative residuals and a
@@ -134,37 +137,69 @@ static int cg64(Grid &g, ops_dat u, ops_dat b, ops_dat r, ops_dat p, ops_dat w, 
   return it;
 }
 
-/* FP32 inner CG on A d = r32 (r32, p32 set, d32 = 0 by the caller) */
-static int cg32(Grid &g, ops_dat d, ops_dat r, ops_dat p, ops_dat w, ops_dat Kx, ops_dat Ky,
-                double rr_in, double tol, int maxit) {
-  double rro = rr_in;
-  const double rr0 = rr_in;
+/* Mixed precision CG: r, w, p in FP32 (FP32 arithmetic, dot products
+ * accumulated in FP64), the iterate x in FP64 and updated in FP64 every
+ * iteration.  When the recursive residual has dropped by `drop` since the
+ * last true residual, or meets tol, the residual is replaced by b - A x
+ * computed in FP64 (reliable updates: the search direction p is kept, so CG
+ * keeps its FP64 convergence) and convergence is tested on that residual.
+ * Returns the CG iterations; *repl counts the FP64 residual evaluations,
+ * *rel the final true relative residual. */
+static int cg_mixed(Grid &g, ops_dat x, ops_dat b, ops_dat r, ops_dat p, ops_dat w,
+                    ops_dat Kx, ops_dat Ky, ops_dat Kx32, ops_dat Ky32, double tol, double drop,
+                    int maxit, int *repl, double *rel) {
+  auto true_res = [&]() {  // r = b - A x in FP64, stored in FP32
+    ops_par_loop(hc_res32_kernel, "hc_res32_kernel", g.blk, 2, g.in,
+                 ops_arg_dat(r, 1, g.S00, "float", OPS_WRITE),
+                 ops_arg_dat(Kx, 1, g.SKX, "double", OPS_READ),
+                 ops_arg_dat(Ky, 1, g.SKY, "double", OPS_READ),
+                 ops_arg_dat(x, 1, g.S5, "double", OPS_READ),
+                 ops_arg_dat(b, 1, g.S00, "double", OPS_READ),
+                 ops_arg_reduce(g.red, 1, "double", OPS_INC));
+    return reduce_result(g);
+  };
+  double rro = true_res();
+  const double rr0 = rro;
+  double rr_true = rro;
+  *repl = 1;
+  *rel = rr0 > 0.0 ? 1.0 : 0.0;
+  ops_par_loop(hc_copy32_kernel, "hc_copy32_kernel", g.blk, 2, g.in,
+               ops_arg_dat(p, 1, g.S00, "float", OPS_WRITE),
+               ops_arg_dat(r, 1, g.S00, "float", OPS_READ));
   int it = 0;
-  while (it < maxit && rro > 0.0 && sqrt(rro / rr0) > tol) {
+  while (it < maxit && rro > 0.0 && *rel > tol) {
     ops_par_loop(hc_w32_kernel, "hc_w32_kernel", g.blk, 2, g.in,
                  ops_arg_dat(w, 1, g.S00, "float", OPS_WRITE),
-                 ops_arg_dat(Kx, 1, g.SKX, "float", OPS_READ),
-                 ops_arg_dat(Ky, 1, g.SKY, "float", OPS_READ),
+                 ops_arg_dat(Kx32, 1, g.SKX, "float", OPS_READ),
+                 ops_arg_dat(Ky32, 1, g.SKY, "float", OPS_READ),
                  ops_arg_dat(p, 1, g.S5, "float", OPS_READ),
                  ops_arg_reduce(g.red, 1, "double", OPS_INC));
     const double pw = reduce_result(g);
-    const float alpha = (float)(rro / pw);
-    ops_par_loop(hc_ur32_kernel, "hc_ur32_kernel", g.blk, 2, g.in,
-                 ops_arg_dat(d, 1, g.S00, "float", OPS_RW),
+    const double alpha = rro / pw;
+    ops_par_loop(hc_xr32_kernel, "hc_xr32_kernel", g.blk, 2, g.in,
+                 ops_arg_dat(x, 1, g.S00, "double", OPS_RW),
                  ops_arg_dat(r, 1, g.S00, "float", OPS_RW),
                  ops_arg_dat(p, 1, g.S00, "float", OPS_READ),
                  ops_arg_dat(w, 1, g.S00, "float", OPS_READ),
-                 ops_arg_gbl(&alpha, 1, "float", OPS_READ),
+                 ops_arg_gbl(&alpha, 1, "double", OPS_READ),
                  ops_arg_reduce(g.red, 1, "double", OPS_INC));
-    const double rnn = reduce_result(g);
+    double rnn = reduce_result(g);
+    it++;
+    if (sqrt(rnn / rr_true) <= drop || sqrt(rnn / rr0) <= tol) {
+      rnn = true_res();
+      rr_true = rnn;
+      (*repl)++;
+      *rel = sqrt(rnn / rr0);
+      if (*rel <= tol) break;
+    }
     const float beta = (float)(rnn / rro);
     ops_par_loop(hc_p32_kernel, "hc_p32_kernel", g.blk, 2, g.in,
                  ops_arg_dat(p, 1, g.S00, "float", OPS_RW),
                  ops_arg_dat(r, 1, g.S00, "float", OPS_READ),
                  ops_arg_gbl(&beta, 1, "float", OPS_READ));
     rro = rnn;
-    it++;
   }
+  if (it >= maxit) *rel = sqrt(true_res() / rr0);
   return it;
 }
 
@@ -172,7 +207,7 @@ int main(int argc, char **argv) {
   ops_init(argc, argv, 1);
   const int N = iopt(argc, argv, "-n=", 4096);
   const double tol = dopt(argc, argv, "-tol=", 1e-10);
-  const double inner = dopt(argc, argv, "-inner=", 1e-4);
+  const double inner = dopt(argc, argv, "-inner=", 1e-2);
   const int maxit = iopt(argc, argv, "-maxit=", 20000);
   const double dt = dopt(argc, argv, "-dt=", 4e-6);
   const char *prec = sopt(argc, argv, "-prec=");
@@ -272,43 +307,25 @@ int main(int argc, char **argv) {
     ops_dat r32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "r32");
     ops_dat p32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "p32");
     ops_dat w32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "w32");
-    ops_dat d32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "d32");
     int all[] = {0, N + 1, 0, N + 1};
     ops_par_loop(hc_coef32_kernel, "hc_coef32_kernel", g.blk, 2, all,
                  ops_arg_dat(Kx32, 1, g.S00, "float", OPS_WRITE),
                  ops_arg_dat(Ky32, 1, g.S00, "float", OPS_WRITE),
                  ops_arg_dat(Kx, 1, g.S00, "double", OPS_READ),
                  ops_arg_dat(Ky, 1, g.S00, "double", OPS_READ));
-    double c0, e0, c1, e1;
+    double c0, e0, c1, e1, rel = 1.0;
+    int repl = 0;
     ops_timers(&c0, &e0);
-    int outer = 0, inner_total = 0;
-    double rr0 = -1.0, rel = 1.0;
-    while (outer < 50) {
-      ops_par_loop(hc_res32_kernel, "hc_res32_kernel", g.blk, 2, g.in,
-                   ops_arg_dat(r32, 1, g.S00, "float", OPS_WRITE),
-                   ops_arg_dat(p32, 1, g.S00, "float", OPS_WRITE),
-                   ops_arg_dat(d32, 1, g.S00, "float", OPS_WRITE),
-                   ops_arg_dat(Kx, 1, g.SKX, "double", OPS_READ),
-                   ops_arg_dat(Ky, 1, g.SKY, "double", OPS_READ),
-                   ops_arg_dat(x64, 1, g.S5, "double", OPS_READ),
-                   ops_arg_dat(b, 1, g.S00, "double", OPS_READ),
-                   ops_arg_reduce(g.red, 1, "double", OPS_INC));
-      const double rr = reduce_result(g);
-      if (rr0 < 0.0) rr0 = rr;
-      rel = rr0 > 0.0 ? sqrt(rr / rr0) : 0.0;
-      if (rel <= tol || inner_total >= maxit) break;
-      inner_total += cg32(g, d32, r32, p32, w32, Kx32, Ky32, rr, inner, maxit - inner_total);
-      ops_par_loop(hc_update_kernel, "hc_update_kernel", g.blk, 2, g.in,
-                   ops_arg_dat(x64, 1, g.S00, "double", OPS_RW),
-                   ops_arg_dat(d32, 1, g.S00, "float", OPS_READ));
-      outer++;
-    }
+    const int it = cg_mixed(g, x64, b, r32, p32, w32, Kx, Ky, Kx32, Ky32, tol, inner, maxit,
+                            &repl, &rel);
     ops_timers(&c1, &e1);
     t32 = e1 - e0;
-    // residual model: 48 B/cell (Kx, Ky, x, b read; r, p, d written as FP32
-    // counts 8+8+8+8+4+4+4), inner 52 B/cell, update 20 B/cell
-    const double bytes = cells * (52.0 * inner_total + 44.0 * (outer + 1) + 20.0 * outer);
-    ops_printf("mixed outer %d  inner %d  true_resid %.15e\n", outer, inner_total, rel);
+    // bytes model per iteration: w = A p reads Kx, Ky, p (FP32) and writes w
+    // (16 B); x += alpha p, r -= alpha w read p, w and update x (FP64) and r
+    // (32 B); p = r + beta p (12 B); each FP64 residual reads Kx, Ky, x, b
+    // and writes r (36 B)
+    const double bytes = cells * (60.0 * it + 36.0 * repl);
+    ops_printf("mixed iterations %d  replacements %d  true_resid %.15e\n", it, repl, rel);
     ops_printf("timing mixed %.6f s  %.1f GB/s\n", t32, bytes / t32 / 1e9);
     ops_printf("mixed checksum %.15e\n", checksum(g, x64));
   }

@@ -9,8 +9,8 @@
  * Kx, Ky zero on the domain faces (no flux through the boundary).
  *
  * The *32 kernels are the mixed-precision form: FP32 storage and arithmetic
- * for the inner CG sweeps, dot products accumulated in FP64, the outer
- * residual and the solution update in FP64.
+ * for the CG vectors, dot products accumulated in FP64, the iterate and the
+ * replacement residual in FP64.
  */
 #ifndef HEAT_CG_KERNELS_H
 #define HEAT_CG_KERNELS_H
@@ -92,20 +92,19 @@ void hc_coef32_kernel(ACC<float> &Kx32, ACC<float> &Ky32, const ACC<double> &Kx,
   Ky32(0, 0) = (float)Ky(0, 0);
 }
 
-/* FP64 residual of the FP64 iterate, stored in FP32 as the inner right-hand
- * side: r32 = p32 = b - A x, d32 = 0, rr += r.r (FP64) */
-void hc_res32_kernel(ACC<float> &r32, ACC<float> &p32, ACC<float> &d32, const ACC<double> &Kx,
-                     const ACC<double> &Ky, const ACC<double> &x, const ACC<double> &b,
-                     double *rr) {
+/* FP64 residual of the FP64 iterate, stored in FP32: r32 = b - A x,
+ * rr += r.r (FP64) */
+void hc_res32_kernel(ACC<float> &r32, const ACC<double> &Kx, const ACC<double> &Ky,
+                     const ACC<double> &x, const ACC<double> &b, double *rr) {
   const double ax = (1.0 + hc_ry * (Ky(0, 1) + Ky(0, 0)) + hc_rx * (Kx(1, 0) + Kx(0, 0))) * x(0, 0) -
                     hc_ry * (Ky(0, 1) * x(0, 1) + Ky(0, 0) * x(0, -1)) -
                     hc_rx * (Kx(1, 0) * x(1, 0) + Kx(0, 0) * x(-1, 0));
   const double rv = b(0, 0) - ax;
   r32(0, 0) = (float)rv;
-  p32(0, 0) = (float)rv;
-  d32(0, 0) = 0.0f;
   *rr = *rr + rv * rv;
 }
+
+void hc_copy32_kernel(ACC<float> &p, const ACC<float> &r) { p(0, 0) = r(0, 0); }
 
 /* w = A p in FP32, pw += p.w accumulated in FP64 */
 void hc_w32_kernel(ACC<float> &w, const ACC<float> &Kx, const ACC<float> &Ky,
@@ -117,11 +116,11 @@ void hc_w32_kernel(ACC<float> &w, const ACC<float> &Kx, const ACC<float> &Ky,
   *pw = *pw + (double)ap * (double)p(0, 0);
 }
 
-/* d += alpha p, r -= alpha w (FP32), rnn += r.r (FP64) */
-void hc_ur32_kernel(ACC<float> &d, ACC<float> &r, const ACC<float> &p, const ACC<float> &w,
-                    const float *alpha, double *rnn) {
-  d(0, 0) = d(0, 0) + (*alpha) * p(0, 0);
-  const float rv = r(0, 0) - (*alpha) * w(0, 0);
+/* x += alpha p in FP64, r -= alpha w in FP32, rnn += r.r (FP64) */
+void hc_xr32_kernel(ACC<double> &x, ACC<float> &r, const ACC<float> &p, const ACC<float> &w,
+                    const double *alpha, double *rnn) {
+  x(0, 0) = x(0, 0) + (*alpha) * (double)p(0, 0);
+  const float rv = r(0, 0) - (float)(*alpha) * w(0, 0);
   r(0, 0) = rv;
   *rnn = *rnn + (double)rv * (double)rv;
 }
@@ -129,8 +128,5 @@ void hc_ur32_kernel(ACC<float> &d, ACC<float> &r, const ACC<float> &p, const ACC
 void hc_p32_kernel(ACC<float> &p, const ACC<float> &r, const float *beta) {
   p(0, 0) = r(0, 0) + (*beta) * p(0, 0);
 }
-
-/* x += d (the FP32 correction applied in FP64) */
-void hc_update_kernel(ACC<double> &x, const ACC<float> &d) { x(0, 0) = x(0, 0) + (double)d(0, 0); }
 
 #endif

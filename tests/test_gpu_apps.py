@@ -145,13 +145,18 @@ def test_heat_cg_fixed_iterations_match_oracle(golden):
     """40 CG iterations without a stopping test, FP64 and mixed: the dats
     against the oracle's.  The dot products are summed in a different order
     (tree vs sequential), so alpha and beta differ in the last bits and the
-    iterates drift apart at round-off: FP64 dats within 1e-10 of the field's
-    scale; FP32 dats within 1e-5 of the field's scale (an FP32 alpha that
-    rounds the other way moves every point by one float ulp)."""
+    iterates drift apart at round-off: the FP64 solver's dats (and the set-up
+    dats) within 1e-10 of the field's scale; the mixed form's dats (FP32
+    vectors and the FP64 iterate they update) within 1e-5 of the field's
+    scale (a beta that rounds to the other float moves every point by one
+    float ulp)."""
     g = golden["reference_runs"]["heat_cg_96_fixed"]
     gout, gd = run_app("heat_cg", "b200", g["args"], dump=True)
     cout, cd = run_app("heat_cg", "oracle", g["args"], dump=True)
-    check_dumps(gd, cd, tol=1e-10, float_tol=1e-5, floor_frac=1.0)
+    diffs = compare(gd, cd, floor_frac=1.0)
+    mixed_form = {"x", "r32", "p32", "w32"}
+    for name, d in diffs.items():
+        assert d <= (1e-5 if name in mixed_form else 1e-10), (name, d)
     got, want = result_lines(gout, HEAT_KEYS), g["lines"]
     assert [words_and_counts(l) for l in got] == [words_and_counts(l) for l in want]
     assert_lines_close(got[:2], want[:2], 1e-9)
