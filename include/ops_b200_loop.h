@@ -56,6 +56,8 @@ typedef struct ob2_loop {
                                kernel loops over the remaining y/z */
   int idx32;                /* 1: every dat has < 2^31 elements, so element
                                offsets fit 32-bit arithmetic */
+  int tune;                 /* >= 0: this launch times block-shape candidate
+                               `tune` of the autotuner (OPS_B200_AUTOTUNE) */
 } ob2_loop;
 
 /* A generated launcher: launches one kernel variant with the parameter block

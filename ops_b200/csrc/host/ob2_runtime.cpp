@@ -16,6 +16,7 @@
 // wait for the device; only reduction results, fetches and host raw pointers
 // synchronise.  Errors surface as OPSException with the reference's codes.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <limits>
@@ -36,7 +37,23 @@ struct KStat {
   double host_s = 0.0;    // host wall time (enqueue, or device time under diags>1)
   double dev_ms = 0.0;    // device time from events (diags > 1)
   double transfer = 0.0;  // bytes, OPS transfer model
+  // block-shape autotuning (loops without reductions): 0 not started,
+  // 1 every candidate launched once, 2 decided
+  int tune_state = 0;
+  int tune_next = 0;
+  int tune_dim = 2;
+  int best[3] = {0, 0, 0};
+  std::vector<void *> tune_ev;        // start/end event per candidate
+  std::vector<long long> tune_pts;    // points of the candidate's launch
 };
+
+// block shapes the autotuner tries (x, y, z); one thread per point, so the
+// shape changes neither any point's arithmetic nor, for loops without
+// reductions, any result
+static const int kTune2[][3] = {{32, 4, 1}, {32, 8, 1}, {64, 4, 1}, {128, 2, 1}, {32, 16, 1},
+                                {256, 1, 1}};
+static const int kTune3[][3] = {{32, 4, 1}, {32, 8, 1}, {64, 4, 1}, {32, 4, 2}, {32, 2, 4}};
+void tune_decide(KStat &k, int dim);
 
 struct DatX {
   int edat_prev_acc = -1;  // last access kind of an edge dat
@@ -96,6 +113,9 @@ struct Runtime {
   bool capturing = false;     // recording a loop chain into a graph
   int max_chain = 64;         // queued items that force a flush (0: no limit)
   int red_waves = 1;          // reduction grids: waves of resident CTAs (OPS_B200_RED_WAVES)
+  bool autotune = false;      // block-shape autotuning (OPS_B200_AUTOTUNE / OPS_AUTOTUNE)
+  std::string tune_file;      // decisions read at ops_init, written at ops_exit
+  std::unordered_map<std::string, std::array<int, 3>> tune_known;
   double cache_mb = 40.0;   // L2 budget per tile (OPS_CACHE_SIZE, MB)
   struct QAcc { int dat; int acc; int rmin, rmax; int flat; };  // no padding: hashed as bytes
   struct QItem {
@@ -257,6 +277,12 @@ int kernel_slot(const char *name) {
   r.kstats.push_back(KStat());
   r.kstats.back().name = name;
   r.kindex[name] = k;
+  auto t = r.tune_known.find(name);
+  if (t != r.tune_known.end()) {
+    KStat &s = r.kstats.back();
+    s.tune_state = 2;
+    for (int i = 0; i < 3; i++) s.best[i] = t->second[i];
+  }
   return k;
 }
 
@@ -516,10 +542,22 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t
   bool reduce = false;
   for (int i = 0; i < L->nargs; i++)
     if (L->red[i].acc) reduce = true;
-  if (!r.lazy || reduce) {
+  if (!r.lazy || reduce || L->tune >= 0) {
     ob2_flush();
     void *ev = kt_begin();
+    void *t0 = nullptr, *t1 = nullptr;
+    if (L->tune >= 0) {
+      t0 = pool_event();
+      ob2_event_record(t0);
+    }
     int e = fn(params, grid, block, L->stream);
+    if (L->tune >= 0) {
+      t1 = pool_event();
+      ob2_event_record(t1);
+      KStat &k = r.kstats[L->kernel_index];
+      k.tune_ev[2 * L->tune] = t0;
+      k.tune_ev[2 * L->tune + 1] = t1;
+    }
     kt_end(ev, L->kernel_index);
     if (e) {
       OPSException ex(OPS_RUNTIME_ERROR);
@@ -590,6 +628,7 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
     if ((p = strstr(a, "OPS_TILESIZE_Y="))) r.tile_y = atoi(p + 15);
     if ((p = strstr(a, "OPS_TILESIZE_Z="))) r.tile_z = atoi(p + 15);
     if ((p = strstr(a, "OPS_CACHE_SIZE="))) r.cache_mb = atof(p + 15);
+    if (strstr(a, "OPS_AUTOTUNE")) r.autotune = true;
   }
   const char *e;
   if ((e = getenv("OPS_B200_LAZY"))) r.lazy = atoi(e) != 0;
@@ -601,6 +640,18 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_CACHE_MB"))) r.cache_mb = atof(e);
   if ((e = getenv("OPS_B200_MAX_CHAIN"))) r.max_chain = atoi(e);
   if ((e = getenv("OPS_B200_RED_WAVES"))) r.red_waves = std::max(1, atoi(e));
+  if ((e = getenv("OPS_B200_AUTOTUNE"))) r.autotune = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
+    r.tune_file = e;
+    if (FILE *f = fopen(e, "r")) {  // decisions of an earlier run
+      char nm[256];
+      int bx, by, bz;
+      while (fscanf(f, "%255s %d %d %d", nm, &bx, &by, &bz) == 4)
+        if (bx > 0 && by > 0 && bz > 0 && bx * by * bz <= 1024)
+          r.tune_known[nm] = {bx, by, bz};
+      fclose(f);
+    }
+  }
   if (r.cache_mb <= 0.0) r.cache_mb = 40.0;
   if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
   if ((e = getenv("OPS_B200_BLOCK"))) sscanf(e, "%d,%d,%d", &r.block_x, &r.block_y, &r.block_z);
@@ -622,6 +673,18 @@ OPS_API void ops_dump_dats(const char *path);
 OPS_API void ops_exit(void) {
   if (!R || !R->initialised) return;
   ob2_flush();
+  Runtime &r = rt();
+  if (r.autotune && !r.tune_file.empty()) {
+    ob2_dev_sync();
+    if (FILE *f = fopen(r.tune_file.c_str(), "w")) {
+      for (auto &k : r.kstats) {
+        if (k.tune_state == 1) tune_decide(k, k.tune_dim);
+        if (k.tune_state == 2)
+          fprintf(f, "%s %d %d %d\n", k.name.c_str(), k.best[0], k.best[1], k.best[2]);
+      }
+      fclose(f);
+    }
+  }
   const char *dump = getenv("OPS_DUMP_FILE");
   if (dump && *dump) ops_dump_dats(dump);
   ob2_dev_sync();
@@ -1094,6 +1157,66 @@ OPS_API void ops_execute(OPS_instance *) { ob2_flush(); }
 /* ------------------------------------------------------------------------
  * par_loop support for generated stubs (loop_host.cpp.j2:13-780)
  * ---------------------------------------------------------------------- */
+/* Block-shape autotuner.  After one untimed launch with the default shape,
+ * each candidate shape is launched kTuneReps times, eagerly and bracketed by
+ * events; at the kernel's next launch the shape with the smallest device
+ * time per point (best of its repetitions) is kept for the rest of the run
+ * (and written to OPS_B200_TUNE_FILE at ops_exit). */
+namespace {
+constexpr int kTuneReps = 2;
+
+int tune_count(int dim) {
+  return dim == 2 ? (int)(sizeof kTune2 / sizeof kTune2[0]) : (int)(sizeof kTune3 / sizeof kTune3[0]);
+}
+
+void tune_decide(KStat &k, int dim) {
+  const int nc = tune_count(dim);
+  std::vector<double> best_per(nc, 1e300);
+  for (int j = 0; j < nc * kTuneReps && 2 * j + 1 < (int)k.tune_ev.size(); j++) {
+    float ms = 0.f;
+    if (!k.tune_ev[2 * j] || ob2_event_elapsed_ms(k.tune_ev[2 * j], k.tune_ev[2 * j + 1], &ms))
+      continue;
+    const double per = ms / (double)std::max(1LL, k.tune_pts[j]);
+    best_per[j % nc] = std::min(best_per[j % nc], per);
+  }
+  int bi = 0;
+  for (int c = 1; c < nc; c++)
+    if (best_per[c] < best_per[bi]) bi = c;
+  const int(*t)[3] = dim == 2 ? kTune2 : kTune3;
+  for (int i = 0; i < 3; i++) k.best[i] = t[bi][i];
+  for (void *e : k.tune_ev)
+    if (e) rt().ev_pool.push_back(e);
+  k.tune_ev.clear();
+  k.tune_state = 2;
+}
+
+void tune_pick(ob2_loop *L) {
+  Runtime &r = rt();
+  KStat &k = r.kstats[L->kernel_index];
+  const int dim = L->dim > 3 ? 3 : L->dim;
+  const int nc = tune_count(dim);
+  const int(*t)[3] = dim == 2 ? kTune2 : kTune3;
+  if (k.tune_state == 1) {
+    ob2_flush();
+    tune_decide(k, dim);
+  }
+  if (k.tune_state == 2) {
+    for (int i = 0; i < 3; i++) L->block[i] = k.best[i];
+    return;
+  }
+  k.tune_dim = dim;
+  if (k.tune_next++ == 0) return;  // first launch: default shape, untimed
+  const int j = k.tune_next - 2;  // timed launch index
+  const int c = j % nc;
+  for (int i = 0; i < 3; i++) L->block[i] = t[c][i];
+  L->tune = j;
+  if ((int)k.tune_ev.size() < 2 * nc * kTuneReps) k.tune_ev.resize(2 * nc * kTuneReps, nullptr);
+  if ((int)k.tune_pts.size() < nc * kTuneReps) k.tune_pts.resize(nc * kTuneReps, 0);
+  k.tune_pts[j] = L->npoints;
+  if (j + 1 == nc * kTuneReps) k.tune_state = 1;
+}
+}  // namespace
+
 OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int dim,
                            const int *range, ops_arg *args, int nargs) {
   require_init();
@@ -1207,6 +1330,8 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   // reduction argument's region is rounded up to 256 bytes by the stub
   // grid: x covers the range; y and z are capped so that the grid is about
   // one wave of resident CTAs (SMs x CTAs per SM), threads loop over the rest
+  L->tune = -1;
+  if (r.autotune && nred == 0 && dim >= 2) tune_pick(L);
   {
     long long tpb = (long long)L->block[0] * L->block[1] * L->block[2];
     long long per_sm = std::max(1LL, 2048 / tpb);
@@ -1384,6 +1509,16 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   }
   snprintf(line, sizeof line, "  Total kernel time (host): %f\n", tt);
   s += line;
+  if (r.autotune) {
+    s += "  Autotuned block shapes:";
+    for (auto &k : r.kstats)
+      if (k.tune_state == 2) {
+        snprintf(line, sizeof line, " %s=%dx%dx%d", k.name.c_str(), k.best[0], k.best[1],
+                 k.best[2]);
+        s += line;
+      }
+    s += "\n";
+  }
   if (r.lazy) {
     snprintf(line, sizeof line,
              "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "

@@ -79,3 +79,35 @@ def test_mblock_halos_lazy_matches_eager(tmp_path):
                            env=dict(os.environ, OPS_DUMP_FILE=dumps[tag], **env), timeout=300)
         assert r.returncode == 0, r.stderr[-2000:]
     same(dumps["lazy"], dumps["eager"])
+
+
+AUTOTUNE = {"OPS_B200_AUTOTUNE": "1"}
+
+
+@pytest.mark.parametrize("app,args", [
+    ("poisson_mb", ["-nb=3", "-n=61", "-sweeps=25", "-check=5"]),
+    ("opsunit", ["-nx=45", "-ny=38"]),
+    ("adi3d", ["-nx=40", "-ny=23", "-nz=17", "-steps=3", "-prec=64"]),
+])
+def test_autotuned_block_shapes_give_identical_results(app, args):
+    """The block-shape autotuner launches each candidate shape once and keeps
+    the fastest; loops without reductions compute every point the same way
+    under any shape (loops with reductions are not tuned), so every dat is
+    bit-identical to the default shape's run."""
+    eo, ed = run_app(app, "b200", args, dump=True, env=EAGER)
+    to, td = run_app(app, "b200", args + ["-OPS_DIAGS=1"], dump=True, env=AUTOTUNE)
+    same(td, ed)
+    assert numbers_only(result_lines(to)) == numbers_only(result_lines(eo))
+
+
+def test_cloverleaf_autotuned_matches_default(tmp_path):
+    ensure("clover_step", "b200")
+    dumps = {}
+    for tag, env in (("default", {}), ("tuned", AUTOTUNE)):
+        dumps[tag] = str(tmp_path / ("%s.dump" % tag))
+        r = subprocess.run([sys.executable, "-m", "apps.clover_run", "--flavour", "b200",
+                            "--cells", "120", "--steps", "12", "--dump", dumps[tag]], cwd=ROOT,
+                           env=dict(os.environ, **env), capture_output=True, text=True,
+                           timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+    same(dumps["tuned"], dumps["default"])
