@@ -19,8 +19,9 @@
 // Lines of up to 32*CL points use one warp per line and PCR with warp
 // shuffles (no shared memory, no CTA barriers).  For strided lines (y, z)
 // the CTA's 8 lines are staged through shared memory so that loads and
-// stores are contiguous runs along x.  Longer lines use a CTA per group of
-// lines with PCR in shared memory.  Each coefficient is read once and the
+// stores are contiguous runs along x (or, on request, one thread per line
+// runs the Thomas algorithm: trid_thomas_kernel).  Longer lines use a CTA per
+// group of lines with PCR in shared memory.  Each coefficient is read once and the
 // solution written once: the DRAM traffic is the algorithmic 5 values per
 // point (7 for _Inc).  Elimination is FP64 for double and float storage.
 // Every register array is indexed with compile-time indices only (a run-time
@@ -28,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
+
+#include <algorithm>
 
 #include "ops_b200_device.h"
 
@@ -318,10 +321,109 @@ __global__ void __launch_bounds__(kThreads) trid_cta_kernel(
     }
 }
 
+// Strided lines (y, z): one thread per line, neighbouring threads on
+// neighbouring lines along the fastest other axis, so every load and store
+// of a warp is one contiguous run.  The Thomas algorithm in FP64 with the
+// operation order of the sequential restatement (c'_i = c_i m_i,
+// d'_i = (d_i - a_i d'_{i-1}) m_i, m_i = 1 / (b_i - a_i c'_{i-1}), then
+// x_i = d'_i - c'_i x_{i+1}), every product and difference rounded on its own
+// (no contraction), so the solution equals the oracle's bit for bit.  The
+// forward sweep keeps c' and d' in a device scratch array laid out
+// [point][line] (coalesced too); the backward sweep reads them back, mostly
+// from L2.  Traffic: the algorithmic 4 reads + 1 write per point, plus the
+// scratch's 2 writes + 2 reads where it leaves L2.
+template <typename T, bool INC>
+__global__ void __launch_bounds__(128) trid_thomas_kernel(
+    int n, long long nlines, long long stride, int o1n, long long o1s, long long o2s,
+    const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
+    T *__restrict__ D, T *__restrict__ U, double *__restrict__ cpd) {
+  for (long long line = (long long)blockIdx.x * blockDim.x + threadIdx.x; line < nlines;
+       line += (long long)gridDim.x * blockDim.x) {
+    const long long base = (line % o1n) * o1s + (line / o1n) * o2s;
+    double *cp = cpd + line, *dp = cpd + (long long)n * nlines + line;
+    double m = __ddiv_rn(1.0, (double)B[base]);
+    double cprev = __dmul_rn((double)C[base], m);
+    double dprev = __dmul_rn((double)D[base], m);
+    cp[0] = cprev;
+    dp[0] = dprev;
+#pragma unroll 4
+    for (int k = 1; k < n; k++) {
+      const long long e = base + (long long)k * stride;
+      const double a = (double)A[e], b = (double)B[e], c = (double)C[e], d = (double)D[e];
+      m = __ddiv_rn(1.0, __dsub_rn(b, __dmul_rn(a, cprev)));
+      cprev = __dmul_rn(c, m);
+      dprev = __dmul_rn(__dsub_rn(d, __dmul_rn(a, dprev)), m);
+      cp[(long long)k * nlines] = cprev;
+      dp[(long long)k * nlines] = dprev;
+    }
+    double x = dprev;
+    {
+      const long long e = base + (long long)(n - 1) * stride;
+      if (INC)
+        U[e] = (T)__dadd_rn((double)U[e], x);
+      else
+        D[e] = (T)x;
+    }
+#pragma unroll 4
+    for (int k = n - 2; k >= 0; k--) {
+      x = __dsub_rn(dp[(long long)k * nlines], __dmul_rn(cp[(long long)k * nlines], x));
+      const long long e = base + (long long)k * stride;
+      if (INC)
+        U[e] = (T)__dadd_rn((double)U[e], x);
+      else
+        D[e] = (T)x;
+    }
+  }
+}
+
 struct Lines {
   int n, unit, o1n;
   long long nlines, stride, o1s, o2s;
 };
+
+// scratch for the Thomas kernel's c' and d' (grown on demand, kept)
+double *g_cpd = nullptr;
+size_t g_cpd_cap = 0;
+
+template <typename T>
+int launch_thomas(const Lines &g, const void *a, const void *b, const void *c, void *d,
+                  void *u) {
+  const size_t need = (size_t)2 * g.n * g.nlines * sizeof(double);
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  if (need > g_cpd_cap) {
+    if (g_cpd) {
+      cudaStreamSynchronize(st);
+      cudaFree(g_cpd);
+      g_cpd = nullptr;
+      g_cpd_cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&g_cpd, need);
+    if (e != cudaSuccess) return (int)e;
+    g_cpd_cap = need;
+  }
+  // a persistent grid: every line in flight at once would keep 16 bytes
+  // per point of scratch live, far beyond L2 for large batches
+  int sms = 148;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  static int mult = -1;
+  if (mult < 0) {
+    const char *env = getenv("OB2_TRID_THOMAS_CTAS");
+    mult = env ? atoi(env) : 4;
+    if (mult < 1) mult = 1;
+  }
+  long long grid = std::min((g.nlines + 127) / 128, (long long)sms * mult);
+  if (u)
+    trid_thomas_kernel<T, true><<<(unsigned)grid, 128, 0, st>>>(
+        g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b, (const T *)c,
+        (T *)d, (T *)u, g_cpd);
+  else
+    trid_thomas_kernel<T, false><<<(unsigned)grid, 128, 0, st>>>(
+        g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b, (const T *)c,
+        (T *)d, (T *)nullptr, g_cpd);
+  return (int)cudaGetLastError();
+}
 
 template <typename T, int CL>
 int launch_warp(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
@@ -384,6 +486,19 @@ int launch_cta(const Lines &g, const void *a, const void *b, const void *c, void
   return (int)cudaGetLastError();
 }
 
+// OB2_TRID_STRIDED: how strided lines are solved: 1 the staged warp-per-line
+// kernel (default; 296 / 410 us for the 256^3 y / z solves), 0 the Thomas
+// kernel (bit-identical to the sequential restatement; 365 / 409 us: its
+// c'/d' scratch traffic and division chain cost more than the PCR)
+bool use_thomas(int unit) {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("OB2_TRID_STRIDED");
+    v = e ? atoi(e) : 1;
+  }
+  return !unit && v == 0;
+}
+
 // OB2_TRID_STAGED: 0 never, 1 always, 2 strided lines only (default)
 bool use_staged(int unit) {
   static int v = -1;
@@ -413,6 +528,7 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   g.stride = strides[solvedim];
   g.unit = g.stride == 1 ? 1 : 0;
   if (g.n <= 0 || g.nlines <= 0) return 0;
+  if (use_thomas(g.unit)) return launch_thomas<T>(g, a, b, c, d, u);
   if (g.n <= 32 * 16) {
     const bool st = use_staged(g.unit);
     if (g.n <= 32 * 4)

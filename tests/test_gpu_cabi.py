@@ -8,6 +8,8 @@ relative (FP64) of an FP64 Thomas solve; FP32 storage within 2 float ulps.
 
 import ctypes as C
 
+import os
+
 import numpy as np
 import pytest
 
@@ -92,7 +94,8 @@ def test_halo_group_3d_many():
 def thomas(a, b, c, d):
     n = len(d)
     cp, dp = np.zeros(n), np.zeros(n)
-    cp[0], dp[0] = c[0] / b[0], d[0] / b[0]
+    m = 1.0 / b[0]  # the oracle's order (oracle/src/oracle_trid.cpp)
+    cp[0], dp[0] = c[0] * m, d[0] * m
     for i in range(1, n):
         m = 1.0 / (b[i] - a[i] * cp[i - 1])
         cp[i], dp[i] = c[i] * m, (d[i] - a[i] * dp[i - 1]) * m
@@ -122,7 +125,7 @@ def np_trid(A, B, Cc, D, U, solvedim, rng_box):
 @pytest.mark.parametrize("solvedim", [0, 1, 2])
 @pytest.mark.parametrize("inc", [False, True])
 @pytest.mark.parametrize("shape", [(33, 7, 5), (7, 40, 3), (5, 6, 300), (2, 4, 3)])
-def test_trid_batch(typ, solvedim, inc, shape):
+def test_trid_batch(typ, solvedim, inc, shape, exact=False):
     from tests import cabi
     L = cabi.lib()
     blk = L.ops_decl_block(3, b"trid")
@@ -153,9 +156,29 @@ def test_trid_batch(typ, solvedim, inc, shape):
     sbox = [box[0] + 1, box[1] + 1, box[2] + 1, box[3] + 1, box[4] + 1, box[5] + 1]
     want = np_trid(vals["a"], vals["b"], vals["c"], vals["d"], vals["u"] if inc else None,
                    solvedim, sbox)
-    if typ == "double":
+    if exact:
+        assert np.array_equal(got, want)
+    elif typ == "double":
         np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-13)
     else:
         np.testing.assert_allclose(got, want, rtol=2.5e-7, atol=1e-6)
     if inc:  # d untouched by the _Inc form
         assert np.array_equal(dats["d"].get_full(), vals["d"])
+
+
+@pytest.mark.parametrize("typ", ["double", "float"])
+@pytest.mark.parametrize("solvedim", [1, 2])
+@pytest.mark.parametrize("inc", [False, True])
+def test_trid_thomas_strided_bit_exact(typ, solvedim, inc):
+    """OB2_TRID_STRIDED=0: strided lines solved one thread per line by the
+    Thomas algorithm in the restatement's operation order without
+    contraction: bit-identical to it (a child process, since the choice is
+    read once per process)."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import tests.test_gpu_cabi as t; "
+            "t.test_trid_batch(%r, %d, %r, (9, 37, 11), exact=True)" %
+            (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), typ, solvedim, inc))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       env=dict(os.environ, OB2_TRID_STRIDED="0"), timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
