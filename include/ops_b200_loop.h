@@ -64,6 +64,12 @@ typedef struct ob2_loop {
  * `params` (which starts with int lo[3], hi[3]: the loop range) on `stream`. */
 typedef int (*ob2_launcher)(const void *params, const unsigned *grid, const unsigned *block,
                             void *stream);
+/* A generated multi-instance launcher: runs n (<= OB2_MULTI_MAX) instances
+ * of one loop in one launch, instance k with params[k]; grid is the largest
+ * instance grid (the launch's z extent is n times grid[2]). */
+#define OB2_MULTI_MAX 8
+typedef int (*ob2_mlauncher)(const void *const *params, int n, const unsigned *grid,
+                             const unsigned *block, void *stream);
 
 /* Launch or queue one par_loop kernel.  Eager mode (OPS_B200_LAZY=0)
  * launches now.  In lazy mode (the default) loops without reductions are
@@ -76,10 +82,14 @@ typedef int (*ob2_launcher)(const void *params, const unsigned *grid, const unsi
  * plain launches).  With OPS_TILING (or OPS_B200_TILING=1) the chain runs
  * tile by tile: skewed tiles along the slowest axis sized for the L2 budget
  * OPS_CACHE_SIZE (MB), the GPU form of the reference's loop-chain tiling,
- * ops_lazy.cpp:380-1187.  rows_per_thread: points each thread covers along y
- * (the grid's y extent is derived from it per tile). */
-OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t psize,
-                        const unsigned *grid, const unsigned *block, int rows_per_thread);
+ * ops_lazy.cpp:380-1187.  Consecutive queued instances of one loop with
+ * no data shared between them (the blocks of a multi-block program) run as
+ * one launch of mfn (may be NULL: loops with reductions).  rows_per_thread:
+ * points each thread covers along y (the grid's y extent is derived from it
+ * per tile). */
+OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const void *params,
+                        size_t psize, const unsigned *grid, const unsigned *block,
+                        int rows_per_thread);
 
 /* Runs everything the lazy queue holds (no-op in eager mode). */
 OPS_API void ob2_flush(void);

@@ -121,6 +121,7 @@ struct Runtime {
   struct QItem {
     int kind;               // 0 par_loop, 1 halo group
     ob2_launcher fn;
+    ob2_mlauncher mfn;      // multi-instance launcher (NULL: none)
     std::vector<char> prm;
     unsigned grid[3], block[3];
     int py, ndim, kidx;
@@ -135,7 +136,8 @@ struct Runtime {
     std::string params;     // parameter blocks the graph was captured with
   };
   std::unordered_map<std::string, Graph> graph_cache;  // key: the chain's shape
-  long long chains = 0, graph_hits = 0, graph_updates = 0, tiles_run = 0;
+  long long chains = 0, graph_hits = 0, graph_updates = 0, tiles_run = 0, multi_launches = 0;
+  bool multi = true;          // run independent instances of a loop in one launch
 };
 
 Runtime *R = nullptr;
@@ -439,6 +441,47 @@ bool tileable(const Runtime::QItem &it) {
   return true;
 }
 
+// two queued loops touch a common dat and one of them writes it
+bool conflict(const Runtime::QItem &a, const Runtime::QItem &b) {
+  for (auto &x : a.acc)
+    for (auto &y : b.acc)
+      if (x.dat == y.dat && (x.acc != OPS_READ || y.acc != OPS_READ)) return true;
+  return false;
+}
+
+// q[i] starts a run of instances of one loop that can share a launch:
+// returns the end of the run (at most OB2_MULTI_MAX, no data shared)
+size_t multi_run(const std::vector<Runtime::QItem> &q, size_t i) {
+  if (!q[i].mfn || !rt().multi) return i + 1;
+  size_t j = i + 1;
+  while (j < q.size() && j - i < OB2_MULTI_MAX && q[j].kind == 0 && q[j].fn == q[i].fn &&
+         q[j].mfn == q[i].mfn && q[j].prm.size() == q[i].prm.size() &&
+         q[j].block[0] == q[i].block[0] && q[j].block[1] == q[i].block[1] &&
+         q[j].block[2] == q[i].block[2]) {
+    bool ok = true;
+    for (size_t k = i; k < j && ok; k++) ok = !conflict(q[k], q[j]);
+    if (!ok) break;
+    j++;
+  }
+  return j;
+}
+
+void run_multi(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
+  Runtime &r = rt();
+  const void *prm[OB2_MULTI_MAX];
+  unsigned g[3] = {0, 0, 0};
+  for (size_t k = i; k < j; k++) {
+    prm[k - i] = q[k].prm.data();
+    for (int d = 0; d < 3; d++) g[d] = std::max(g[d], q[k].grid[d]);
+  }
+  void *ev = r.capturing ? nullptr : kt_begin();
+  check(q[i].mfn(prm, (int)(j - i), g, q[i].block, ob2_dev_stream()),
+        "ops_par_loop launch (instances)");
+  r.launches++;
+  r.multi_launches++;
+  kt_end(ev, q[i].kidx);
+}
+
 void run_queue(std::vector<Runtime::QItem> &q) {
   Runtime &r = rt();
   size_t i = 0;
@@ -448,6 +491,14 @@ void run_queue(std::vector<Runtime::QItem> &q) {
       while (j < q.size() && tileable(q[j]) && q[j].ndim == q[i].ndim) j++;
       if (j - i >= 2) {
         run_tiled(q, i, j);
+        i = j;
+        continue;
+      }
+    }
+    if (q[i].kind == 0) {
+      const size_t j = multi_run(q, i);
+      if (j - i >= 2) {
+        run_multi(q, i, j);
         i = j;
         continue;
       }
@@ -485,6 +536,7 @@ OPS_API void ob2_flush(void) {
   for (auto &it : q) {
     put(&it.kind, sizeof it.kind);
     put(&it.fn, sizeof it.fn);
+    put(&it.mfn, sizeof it.mfn);
     const size_t np = it.prm.size();
     put(&np, sizeof np);
     put(it.grid, sizeof it.grid);
@@ -536,8 +588,9 @@ OPS_API void ob2_flush(void) {
   check(ob2_graph_launch(G.exec), "loop-chain graph launch");
 }
 
-OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t psize,
-                        const unsigned *grid, const unsigned *block, int rows_per_thread) {
+OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const void *params,
+                        size_t psize, const unsigned *grid, const unsigned *block,
+                        int rows_per_thread) {
   Runtime &r = rt();
   bool reduce = false;
   for (int i = 0; i < L->nargs; i++)
@@ -571,6 +624,7 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, const void *params, size_t
   Runtime::QItem it;
   it.kind = 0;
   it.fn = fn;
+  it.mfn = mfn;
   it.prm.assign((const char *)params, (const char *)params + psize);
   for (int i = 0; i < 3; i++) {
     it.grid[i] = grid[i];
@@ -641,6 +695,7 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_MAX_CHAIN"))) r.max_chain = atoi(e);
   if ((e = getenv("OPS_B200_RED_WAVES"))) r.red_waves = std::max(1, atoi(e));
   if ((e = getenv("OPS_B200_AUTOTUNE"))) r.autotune = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_MULTI"))) r.multi = atoi(e) != 0;
   if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
     r.tune_file = e;
     if (FILE *f = fopen(e, "r")) {  // decisions of an earlier run
@@ -1101,6 +1156,7 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
     Runtime::QItem it;
     it.kind = 1;
     it.fn = nullptr;
+    it.mfn = nullptr;
     for (int i = 0; i < 3; i++) it.grid[i] = it.block[i] = 1, it.lo[i] = it.hi[i] = 0;
     it.py = 1;
     it.ndim = 0;
@@ -1522,8 +1578,8 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   if (r.lazy) {
     snprintf(line, sizeof line,
              "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "
-             "%lld tile launches\n",
-             r.chains, r.graph_hits, r.graph_updates, r.tiles_run);
+             "%lld tile launches, %lld multi-instance launches\n",
+             r.chains, r.graph_hits, r.graph_updates, r.tiles_run, r.multi_launches);
     s += line;
   }
   if (buf && n) {

@@ -633,8 +633,18 @@ class Translator:
         w("template <bool RESTRICT, bool IDX32>")
         minb = self.minb if not reds else 0
         lb = "512, %d" % minb if minb > 0 else "512"
-        w("__global__ void __launch_bounds__(%s) %s(const __grid_constant__ %s p) {" % (lb, K, P))
-        w("  const int x = p.lo0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);")
+        BF = "ob2b_" + loop.stub[len("ops_par_loop_"):]
+        if reds:
+            w("__global__ void __launch_bounds__(%s) %s(const __grid_constant__ %s p) {" %
+              (lb, K, P))
+            w("  const unsigned bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;")
+        else:
+            # the body takes its CTA coordinates as arguments, so that one
+            # launch can also run several instances of this loop (blocks of a
+            # multi-block program) side by side: kernel <K>M below
+            w("static __device__ __forceinline__ void %s(const %s &p, unsigned bx, unsigned by,"
+              " unsigned bz) {" % (BF, P))
+        w("  const int x = p.lo0 + (int)(bx * blockDim.x + threadIdx.x);")
         for i, a, p in reds:
             w("  %s red%d[%s];" % (p.base_type, i, a.dim))
             w("  for (int d = 0; d < (%s); d++) red%d[d] = ob2::identity<%s, %s>();" %
@@ -650,9 +660,9 @@ class Translator:
             # together
             w("  if (x < p.hi0) {")
             w("    const int ys = (int)(gridDim.y * blockDim.y) * %d;" % py)
-            w("    for (int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z); z < p.hi2;"
+            w("    for (int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z); z < p.hi2;"
               " z += (int)(gridDim.z * blockDim.z))")
-            w("      for (int yb = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y) * %d;"
+            w("      for (int yb = p.lo1 + (int)(by * blockDim.y + threadIdx.y) * %d;"
               " yb < p.hi1; yb += ys) {" % py)
             # PY consecutive rows per trip; all in range: no branch between
             # the calls, so the loads of every row can be issued before the
@@ -674,8 +684,8 @@ class Translator:
             w("  }")
         else:
             # PY points per thread along y (consecutive rows), x / z one each
-            w("  const int y0 = p.lo1 + (int)(blockIdx.y * blockDim.y + threadIdx.y) * %d;" % py)
-            w("  const int z = p.lo2 + (int)(blockIdx.z * blockDim.z + threadIdx.z);")
+            w("  const int y0 = p.lo1 + (int)(by * blockDim.y + threadIdx.y) * %d;" % py)
+            w("  const int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z);")
             w("  if (x < p.hi0 && z < p.hi2) {")
             if py == 1:
                 w("    if (y0 < p.hi1) {")
@@ -711,9 +721,40 @@ class Translator:
             w("    ob2::reset_counter(p.counter);")
             w("  }")
         w("}")
+        if not reds:
+            w("template <bool RESTRICT, bool IDX32>")
+            w("__global__ void __launch_bounds__(%s) %s(const __grid_constant__ %s p) {" %
+              (lb, K, P))
+            w("  %s<RESTRICT, IDX32>(p, blockIdx.x, blockIdx.y, blockIdx.z);" % BF)
+            w("}")
+            # several instances in one launch: instance it takes the grid's z
+            # slab [it * gz, (it + 1) * gz); CTAs past an instance's own range
+            # find no points
+            w("struct %sM { %s p[OB2_MULTI_MAX]; unsigned gz; };" % (P, P))
+            w("template <bool RESTRICT, bool IDX32>")
+            w("__global__ void __launch_bounds__(%s) %sM(const __grid_constant__ %sM m) {" %
+              (lb, K, P))
+            w("  const unsigned it = blockIdx.z / m.gz;")
+            w("  %s<RESTRICT, IDX32>(m.p[it], blockIdx.x, blockIdx.y, blockIdx.z - it * m.gz);" %
+              BF)
+            w("}")
         # launchers: the runtime launches a loop now or, in lazy mode, later
         # (possibly once per tile, possibly inside a graph capture)
         LN = "ob2l_" + loop.stub[len("ops_par_loop_"):]
+        MN = "ob2m_" + loop.stub[len("ops_par_loop_"):]
+        if not reds:
+            for rs, ix in (("false", "false"), ("false", "true"), ("true", "false"),
+                           ("true", "true")):
+                w("static int %s_%s_%s(const void *const *prm, int n, const unsigned *g,"
+                  " const unsigned *b, void *st) {" % (MN, rs[0], ix[0]))
+                w("  if (n < 1 || n > OB2_MULTI_MAX) return (int)cudaErrorInvalidValue;")
+                w("  %sM m;" % P)
+                w("  for (int k = 0; k < n; k++) m.p[k] = *(const %s *)prm[k];" % P)
+                w("  m.gz = g[2];")
+                w("  %sM<%s, %s><<<dim3(g[0], g[1], g[2] * n), dim3(b[0], b[1], b[2]), 0,"
+                  " (cudaStream_t)st>>>(m);" % (K, rs, ix))
+                w("  return (int)cudaGetLastError();")
+                w("}")
         for rs, ix in (("false", "false"), ("false", "true"), ("true", "false"), ("true", "true")):
             w("static int %s_%s_%s(const void *prm, const unsigned *g, const unsigned *b,"
               " void *st) {" % (LN, rs[0], ix[0]))
@@ -769,7 +810,12 @@ class Translator:
         w("  const ob2_launcher fn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
           " : (L.idx32 ? %s_t_t : %s_t_f);" % (LN, LN, LN, LN))
         w("  const unsigned g3[3] = {grd.x, grd.y, grd.z}, b3[3] = {blk.x, blk.y, blk.z};")
-        w("  ob2_launch(&L, fn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
+        if reds:
+            w("  const ob2_mlauncher mfn = nullptr;")
+        else:
+            w("  const ob2_mlauncher mfn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
+              " : (L.idx32 ? %s_t_t : %s_t_f);" % (MN, MN, MN, MN))
+        w("  ob2_launch(&L, fn, mfn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")
         w("}")
         w("namespace ob2_%s {" % ns)

@@ -22,6 +22,7 @@ pytestmark = pytest.mark.gpu
 EAGER = {"OPS_B200_LAZY": "0", "OPS_B200_TILING": "0"}
 MODES = {
     "lazy_graphs": {"OPS_B200_LAZY": "1", "OPS_B200_TILING": "0", "OPS_B200_GRAPHS": "1"},
+    "lazy_single": {"OPS_B200_LAZY": "1", "OPS_B200_MULTI": "0", "OPS_B200_GRAPHS": "0"},
     "tiled_plain": {"OPS_B200_TILING": "1", "OPS_B200_GRAPHS": "0", "OPS_B200_TILESIZE_Y": "7",
                     "OPS_B200_TILESIZE_Z": "3"},
     "tiled_graphs": {"OPS_B200_TILING": "1", "OPS_B200_GRAPHS": "1", "OPS_B200_TILESIZE_Y": "5",
