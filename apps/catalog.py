@@ -44,6 +44,21 @@ APPS = {
     "ref_mblock": ("ref", os.path.join(REF, "apps", "c", "mblock"), ["mblock.cpp"], None),
     "ref_laplace": ("ref", os.path.join(REF, "apps", "c", "laplace2d_tutorial", "step7"),
                     ["laplace2d.cpp"], None),
+    # further reference applications, built unchanged (the v2 ACC API)
+    "ref_lowdim": ("ref", os.path.join(REF, "apps", "c", "lowdim_test"), ["lowdim.cpp"], None),
+    "ref_multidim3d": ("ref", os.path.join(REF, "apps", "c", "multiDim3D"), ["multidim.cpp"],
+                       None),
+    "ref_shsgc": ("ref", os.path.join(REF, "apps", "c", "shsgc"), ["shsgc.cpp"], None),
+    "ref_compact": ("ref", os.path.join(REF, "apps", "c", "compact_scheme"),
+                    ["compact_scheme.cpp"], None),
+    "ref_random": ("ref", os.path.join(REF, "apps", "c", "random"), ["random.cpp"], None),
+    "ref_tiling_fix": ("ref", os.path.join(REF, "apps", "c", "tiling_fix"), ["minisenga.cpp"],
+                       None),
+    "ref_adi_burger": ("ref", os.path.join(REF, "apps", "c", "adi_burger"), ["adi_burger.cpp"],
+                       None),
+    "ref_adi_burger3d": ("ref", os.path.join(REF, "apps", "c", "adi_burger_3D"),
+                         ["adi_burger_3D.cpp"], None),
+    "ref_tti": ("ref", os.path.join(REF, "apps", "c", "tti"), ["tti.cpp"], None),
     "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
                    CLOVER_SRCS[:15]),
     # the CloverLeaf step harness: the CloverLeaf sources plus apps/clover_step

@@ -108,6 +108,11 @@ OB2_API int ob2_box_copy(char *dat, int type_size, int ncomp, int soa, const int
 
 /* ---- fills ---- */
 OB2_API int ob2_fill_value(void *p, const void *val, int type_size, size_t count);
+/* smallest key of a NaN element (key = point * ncomp + component; elements
+ * are SoA when soa != 0, AoS otherwise) into *first, or -1 when none;
+ * type_size 8 (double) or 4 (float) */
+OB2_API int ob2_nan_find(const void *p, int type_size, int ncomp, int soa, size_t count,
+                         long long *first);
 /* counter-based uniform / normal stream (splitmix64 of seed and index);
  * type_size 8 (double) or 4 (float) */
 OB2_API int ob2_fill_random(void *p, int type_size, size_t count, unsigned long long seed,

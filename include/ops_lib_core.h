@@ -298,6 +298,13 @@ OPS_API void ops_print_dat_to_txtfile(ops_dat dat, const char *file_name);
 OPS_API void ops_get_data(ops_dat dat);
 OPS_API void ops_put_data(ops_dat dat);
 OPS_API int ops_is_root(void);
+/* process rank and count (ops_dummy_singlenode.cpp:200-202: 0 and 1) */
+OPS_API int ops_get_proc(void);
+OPS_API int ops_num_procs(void);
+/* Stops the program (exit status 2) with the index of the first NaN in a
+ * float or double dat (ops_internal2.h:219, ops_dummy_singlenode.cpp:871-878;
+ * the search runs on the device). */
+OPS_API void ops_NaNcheck(ops_dat dat);
 OPS_API void ops_partition(const char *routine);
 /* External access (ops_lib_core.h:1092-1296) */
 OPS_API int ops_dat_get_local_npartitions(ops_dat dat);

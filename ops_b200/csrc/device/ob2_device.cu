@@ -8,6 +8,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+
 #include "ops_b200_device.h"
 
 namespace {
@@ -305,6 +307,48 @@ __global__ void random_kernel(char *p, int ts, size_t count, unsigned long long 
 }
 
 }  // namespace
+
+namespace {
+template <typename T>
+__global__ void nan_find_kernel(const T *__restrict__ p, int ncomp, int soa, size_t count,
+                                unsigned long long *first) {
+  const size_t npts = count / (size_t)ncomp;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < count;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const T v = p[e];
+    if (v != v) {
+      const unsigned long long key =
+          soa ? (unsigned long long)(e % npts) * ncomp + e / npts : (unsigned long long)e;
+      atomicMin(first, key);
+    }
+  }
+}
+}  // namespace
+
+OB2_API int ob2_nan_find(const void *p, int ts, int ncomp, int soa, size_t count,
+                         long long *first) {
+  *first = -1;
+  if (count == 0 || ncomp < 1) return 0;
+  if (ts != 8 && ts != 4) return (int)cudaErrorInvalidValue;
+  unsigned long long *d = nullptr, h = ~0ULL;
+  cudaError_t e = cudaMallocAsync(&d, sizeof(h), g_stream);
+  if (e != cudaSuccess) return rc(e);
+  e = cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, g_stream);
+  const unsigned blocks = (unsigned)std::min<size_t>((count + 255) / 256, (size_t)g_sms * 8);
+  if (e == cudaSuccess) {
+    if (ts == 8)
+      nan_find_kernel<double><<<blocks, 256, 0, g_stream>>>((const double *)p, ncomp, soa, count, d);
+    else
+      nan_find_kernel<float><<<blocks, 256, 0, g_stream>>>((const float *)p, ncomp, soa, count, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, g_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+  cudaFreeAsync(d, g_stream);
+  if (e != cudaSuccess) return rc(e);
+  *first = h == ~0ULL ? -1 : (long long)h;
+  return 0;
+}
 
 OB2_API int ob2_fill_value(void *p, const void *val, int ts, size_t count) {
   if (count == 0) return 0;

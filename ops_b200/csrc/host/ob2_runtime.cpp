@@ -1609,6 +1609,33 @@ OPS_API void ops_timers(double *cpu, double *et) {
   ops_timers_core(cpu, et);
 }
 OPS_API int ops_is_root(void) { return 1; }
+OPS_API int ops_get_proc(void) { return 0; }
+OPS_API int ops_num_procs(void) { return 1; }
+OPS_API void ops_NaNcheck(ops_dat d) {
+  require_init();
+  ops_printf("ops_NaNcheck_core called for %s \n", d->name);
+  if (strcmp(d->type, "double") && strcmp(d->type, "float")) return;
+  ob2_flush();
+  put_data(d);
+  long long first = -1;
+  check(ob2_nan_find(d->data_d, d->type_size, d->dim, rt().inst.OPS_soa, d->mem / d->type_size,
+                     &first),
+        "ops_NaNcheck");
+  if (first < 0) return;
+  const int comp = (int)(first % d->dim);
+  long long pt = first / d->dim;
+  int idx[OPS_MAX_DIM] = {0};
+  for (int i = 0; i < OPS_MAX_DIM; i++) {
+    const int sz = std::max(1, d->size[i]);
+    idx[i] = (int)(pt % sz) + d->d_m[i];
+    pt /= sz;
+  }
+  printf("Error: NaN detected at element dim:%d,index:(%d", comp, idx[0]);
+  for (int i = 1; i < d->block->dims; i++) printf(",%d", idx[i]);
+  printf(")\n");
+  fflush(stdout);
+  exit(2);
+}
 OPS_API void ops_partition(const char *) {}
 OPS_API void ops_partition_opts_c(const char *) {}
 OPS_API void ops_get_data(ops_dat d) { get_data(d); }

@@ -228,7 +228,7 @@ def parse_params(ptext: str) -> List[KernelParam]:
         if not p or p == "void":
             continue
         t = re.sub(r"\s+", " ", p.strip())
-        m = re.match(r"^(const\s+)?ACC\s*<\s*([\w\s:]+?)\s*>\s*&\s*(\w+)$", t)
+        m = re.match(r"^(const\s+)?ACC\s*<\s*([\w\s:]+?)\s*>\s*&?\s*(\w+)$", t)
         if m:
             out.append(KernelParam(p, m.group(2).strip(), True, bool(m.group(1)), m.group(3)))
             continue

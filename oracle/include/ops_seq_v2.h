@@ -28,6 +28,7 @@
 #include <utility>
 
 #include "ops_lib_core.h"
+#include "ops_tridiag.h"
 
 /* oracle runtime hooks (oracle/src/oracle_core.cpp) */
 OPS_API void oracle_loop_prologue(const char *name, ops_block block, int dim, const int *range,
@@ -90,6 +91,12 @@ template <typename T> struct pick<ACC<T> &> {
   typedef acc_holder<T> type;
 };
 template <typename T> struct pick<const ACC<T> &> {
+  typedef acc_holder<T> type;
+};
+template <typename T> struct pick<ACC<T>> {  // ACC taken by value
+  typedef acc_holder<T> type;
+};
+template <typename T> struct pick<const ACC<T>> {
   typedef acc_holder<T> type;
 };
 

@@ -12,6 +12,8 @@
  * through ops_dat_fetch_data and the dump hook, which is how results are
  * compared.
  */
+#include <string.h>
+
 #include <algorithm>
 #include <chrono>
 #include <limits>
@@ -533,6 +535,36 @@ OPS_API void ops_timers_core(double *cpu, double *et) {
 }
 OPS_API void ops_timers(double *cpu, double *et) { ops_timers_core(cpu, et); }
 OPS_API int ops_is_root(void) { return 1; }
+OPS_API int ops_get_proc(void) { return 0; }
+OPS_API int ops_num_procs(void) { return 1; }
+/* ops_dummy_singlenode.cpp:871-878 / ops_lib_core.cpp:1845-1936: the first
+ * NaN in (point, component) order stops the program with status 2 */
+OPS_API void ops_NaNcheck(ops_dat d) {
+  ops_printf("ops_NaNcheck_core called for %s \n", d->name);
+  const bool dbl = !strcmp(d->type, "double"), flt = !strcmp(d->type, "float");
+  if (!dbl && !flt) return;
+  size_t npts = 1;
+  for (int i = 0; i < OPS_MAX_DIM; i++) npts *= (size_t)std::max(1, d->size[i]);
+  for (size_t pt = 0; pt < npts; pt++)
+    for (int c = 0; c < d->dim; c++) {
+      const size_t e = st().inst.OPS_soa ? pt + (size_t)c * npts : pt * d->dim + c;
+      const double v = dbl ? ((const double *)d->data)[e] : ((const float *)d->data)[e];
+      if (v != v) {
+        int idx[OPS_MAX_DIM];
+        size_t q = pt;
+        for (int i = 0; i < OPS_MAX_DIM; i++) {
+          const int sz = std::max(1, d->size[i]);
+          idx[i] = (int)(q % sz) + d->d_m[i];
+          q /= sz;
+        }
+        printf("Error: NaN detected at element dim:%d,index:(%d", c, idx[0]);
+        for (int i = 1; i < d->block->dims; i++) printf(",%d", idx[i]);
+        printf(")\n");
+        fflush(stdout);
+        exit(2);
+      }
+    }
+}
 OPS_API void ops_partition(const char *) {}
 OPS_API void ops_partition_opts_c(const char *) {}
 OPS_API void ops_get_data(ops_dat) {}

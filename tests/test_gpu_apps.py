@@ -177,3 +177,53 @@ def test_heat_cg_converged_matches_reference(golden):
         assert_lines_close(a, b, 1e-11)
     rel = [float(l.split()[-1]) for l in got if l.startswith("fp64 it")][0]
     assert rel <= 1e-10
+
+
+# further reference applications, built unchanged from the reference tree:
+# (catalog name, arguments, dump comparison, text the application prints when
+# its own check passes)
+REF_APPS = [
+    ("ref_lowdim", [], "exact", "All checks PASSED"),
+    ("ref_multidim3d", [], "exact", "This run is considered PASSED"),
+    ("ref_shsgc", [], "libm", "This run is considered PASSED"),
+    ("ref_random", [], None, "This run is considered PASSED"),
+    ("ref_compact", [], "roundoff", "Successful exit from OPS"),
+    ("ref_adi_burger", [], "roundoff", "Successful exit from OPS"),
+    ("ref_adi_burger3d", [], "roundoff", "Successful exit from OPS"),
+    ("ref_tti", ["24", "20", "16"], "exact", "ops_NaNcheck_core called for ut0"),
+]
+
+
+@pytest.mark.parametrize("name,args,mode,text", REF_APPS, ids=[a[0] for a in REF_APPS])
+def test_more_reference_apps_match_oracle(tmp_path, name, args, mode, text):
+    """Reference applications compiled unchanged by this backend's translator
+    against the same applications on the CPU oracle: every dat (halos
+    included) bit-exact ("exact"), or at round-off of the field's scale where
+    the application solves tridiagonal systems ("roundoff": chunked PCR
+    elimination order, 1e-12 of max|field|); the application's own pass
+    message on the GPU run.  ref_random fills dats from a counter-based
+    stream that differs from the CPU's by design, so only its own
+    statistical check is asserted.  ref_shsgc's kernels call pow and sin,
+    whose CUDA and glibc implementations may differ in the last ulp; its
+    shock-capturing limiter amplifies that over the run ("libm": 1e-6 of the
+    field's scale), and its own RMS check against the expected solution
+    passes on the GPU."""
+    import subprocess
+    from tests.apprun import ensure
+    dumps = {}
+    outs = {}
+    for fl in ("b200", "oracle"):
+        exe = ensure(name, fl, shared=False)
+        dumps[fl] = str(tmp_path / ("%s.dump" % fl))
+        r = subprocess.run([exe, *args], cwd=str(tmp_path), capture_output=True, text=True,
+                           env=dict(os.environ, OPS_DUMP_FILE=dumps[fl]), timeout=600)
+        assert r.returncode == 0, (fl, r.stdout[-1500:], r.stderr[-1500:])
+        outs[fl] = r.stdout
+    assert text in outs["b200"], outs["b200"][-1500:]
+    if mode == "exact":
+        diffs = compare(dumps["b200"], dumps["oracle"])
+        assert max(diffs.values()) == 0.0, {k: v for k, v in diffs.items() if v}
+    elif mode == "roundoff":
+        check_dumps(dumps["b200"], dumps["oracle"], tol=1e-12, float_tol=1e-6, floor_frac=1.0)
+    elif mode == "libm":
+        check_dumps(dumps["b200"], dumps["oracle"], tol=1e-6, float_tol=1e-5, floor_frac=1.0)
