@@ -7,7 +7,8 @@
  * loops, optional arguments (enabled and disabled), RW access with a global
  * constant, an empty range, and low-dim accumulation with combine_inc.
  *
- * Options: -nx= -ny= (default 37 x 23)
+ * Options: -nx= -ny= (default 37 x 23), -soa=1 (SoA storage of multi-component
+ * dats)
  */
 #include <math.h>
 #include <stdio.h>
@@ -31,6 +32,8 @@ static int opt(int argc, char **argv, const char *key, int def) {
 
 int main(int argc, char **argv) {
   ops_init(argc, argv, 1);
+  // -soa=1: multi-component dats stored component-major (ops_set_soa)
+  if (opt(argc, argv, "-soa=", 0)) ops_set_soa(1);
   const int nx = opt(argc, argv, "-nx=", 37), ny = opt(argc, argv, "-ny=", 23);
   ou_scale = 0.75;
   ops_decl_const("ou_scale", 1, "double", &ou_scale);

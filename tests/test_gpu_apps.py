@@ -35,7 +35,8 @@ def check_dumps(gpu_dump, cpu_dump, tol=1e-12, float_tol=1e-6, skip=(), floor_fr
     return diffs
 
 
-@pytest.mark.parametrize("args", [[], ["-nx=29", "-ny=17"], ["-nx=130", "-ny=7"]])
+@pytest.mark.parametrize("args", [[], ["-nx=29", "-ny=17"], ["-nx=130", "-ny=7"],
+                                  ["-nx=31", "-ny=19", "-soa=1"]])
 def test_opsunit_parity(args, golden):
     gout, gd = run_app("opsunit", "b200", args, dump=True)
     cout, cd = run_app("opsunit", "oracle", args, dump=True)
