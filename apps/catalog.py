@@ -34,6 +34,17 @@ CLOVER_SRCS = ["clover_leaf.cpp", "initialise_chunk.cpp", "generate.cpp", "ideal
                "advec_mom.cpp", "reset_field.cpp", "start.cpp", "time_step.cpp",
                "build_field.cpp", "read_input.cpp", "initialise.cpp", "advection.cpp"]
 
+TEALEAF_SRCS = ["tea_leaf.cpp", "field_summary.cpp", "generate.cpp", "initialise_chunk.cpp",
+                "start.cpp", "set_field.cpp", "tea_leaf_cg.cpp", "tea_leaf_cheby.cpp",
+                "tea_leaf_common.cpp", "tea_leaf_jacobi.cpp", "tea_leaf_ppcg.cpp",
+                "update_halo.cpp", "build_field.cpp", "diffuse.cpp", "initialise.cpp",
+                "read_input.cpp", "tea_solve.cpp", "timestep.cpp"]
+CLOVER3D_SRCS = ["clover_leaf.cpp", "initialise_chunk.cpp", "generate.cpp", "ideal_gas.cpp",
+                 "update_halo.cpp", "field_summary.cpp", "viscosity.cpp", "calc_dt.cpp",
+                 "PdV.cpp", "revert.cpp", "accelerate.cpp", "flux_calc.cpp", "advec_cell.cpp",
+                 "advec_mom.cpp", "reset_field.cpp", "start.cpp", "time_step.cpp",
+                 "build_field.cpp", "read_input.cpp", "initialise.cpp", "advection.cpp"]
+
 # name -> (kind, source dir, sources, translated sources (legacy translator))
 APPS = {
     "poisson_mb": ("own", os.path.join(ROOT, "apps", "poisson_mb"), ["poisson_mb.cpp"], None),
@@ -59,6 +70,11 @@ APPS = {
     "ref_adi_burger3d": ("ref", os.path.join(REF, "apps", "c", "adi_burger_3D"),
                          ["adi_burger_3D.cpp"], None),
     "ref_tti": ("ref", os.path.join(REF, "apps", "c", "tti"), ["tti.cpp"], None),
+    # reference applications written with the original OPS_ACCn kernel API
+    # (b200 flavour only: the oracle restates the ACC<> API)
+    "ref_tealeaf": ("ref", os.path.join(REF, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
+    "ref_cloverleaf3d": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
+                         None),
     "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
                    CLOVER_SRCS[:15]),
     # the CloverLeaf step harness: the CloverLeaf sources plus apps/clover_step

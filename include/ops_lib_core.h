@@ -341,6 +341,18 @@ enum {
 };
 #ifdef __cplusplus
 OPS_API bool ops_checkpointing_init(const char *filename, double interval, int options);
+/* the rest of the checkpointing API as in the reference's build without
+ * checkpointing (ops_checkpointing.cpp, #else branch): no data is saved,
+ * "fast forward" never happens, every loop runs */
+OPS_API bool ops_checkpointing_before(ops_arg *args, int nargs, int *range, int loop_id);
+OPS_API bool ops_checkpointing_name_before(ops_arg *args, int nargs, int *range,
+                                           const char *s);
+OPS_API void ops_checkpointing_manual_datlist(int ndats, ops_dat *datlist);
+OPS_API bool ops_checkpointing_fastfw(int nbytes, char *payload);
+OPS_API bool ops_checkpointing_manual_datlist_fastfw(int ndats, ops_dat *datlist, int nbytes,
+                                                     char *payload);
+OPS_API bool ops_checkpointing_manual_datlist_fastfw_trigger(int ndats, ops_dat *datlist,
+                                                             int nbytes, char *payload);
 #endif
 /* HDF5 output (ops_hdf5.h:130-166): this backend has no HDF5; the calls
  * report that on stderr and write nothing. */

@@ -641,7 +641,7 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
   const int td = L->dim - 1;
   for (int i = 0; i < L->nargs; i++) {
     ops_arg &a = L->args[i];
-    if (a.argtype != OPS_ARG_DAT || !a.opt || !a.dat) continue;
+    if (a.argtype != OPS_ARG_DAT || !a.dat) continue;
     Runtime::QAcc qa;
     qa.dat = a.dat->index;
     qa.acc = a.acc;
@@ -1311,7 +1311,10 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
     L->red[i].first = 0;
     L->red[i].op = 0;
     if (a.argtype == OPS_ARG_DAT) {
-      if (!a.opt || !a.dat) continue;
+      // a disabled optional argument (ops_arg_dat_opt, flag 0) still gets
+      // its dat's view when it names one, as in the reference's generated
+      // code, where the flag only matters to distributed halo exchanges
+      if (!a.dat) continue;
       ops_dat d = a.dat;
       if (d->locked_hd) {
         OPSException ex(OPS_INVALID_ARGUMENT);
@@ -1323,7 +1326,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
       // low-dim accumulation: first INC/MIN/MAX since another access fills
       // the dat with the identity (ops_dummy_singlenode.cpp:235-391)
       DatX &dx = r.datx[d->index];
-      if (d->e_dat && (a.acc == OPS_INC || a.acc == OPS_MIN || a.acc == OPS_MAX) &&
+      if (a.opt && d->e_dat && (a.acc == OPS_INC || a.acc == OPS_MIN || a.acc == OPS_MAX) &&
           dx.edat_prev_acc != a.acc) {
         dx.edat_prev_acc = a.acc;
         ob2_flush();
@@ -1430,9 +1433,9 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
 
 OPS_API int ob2_args_alias(const ops_arg *args, int nargs) {
   for (int i = 0; i < nargs; i++) {
-    if (args[i].argtype != OPS_ARG_DAT || !args[i].opt || !args[i].dat) continue;
+    if (args[i].argtype != OPS_ARG_DAT || !args[i].dat) continue;
     for (int j = i + 1; j < nargs; j++) {
-      if (args[j].argtype != OPS_ARG_DAT || !args[j].opt || args[j].dat != args[i].dat) continue;
+      if (args[j].argtype != OPS_ARG_DAT || args[j].dat != args[i].dat) continue;
       if (args[i].acc != OPS_READ || args[j].acc != OPS_READ) return 1;
     }
   }
@@ -1459,7 +1462,7 @@ OPS_API void ob2_loop_end(ob2_loop *L) {
   s.host_s += wall() - L->host_t0;
   for (int i = 0; i < L->nargs; i++) {
     ops_arg &a = L->args[i];
-    if (a.argtype != OPS_ARG_DAT || !a.opt || !a.dat) continue;
+    if (a.argtype != OPS_ARG_DAT || !a.dat) continue;
     ops_dat d = a.dat;
     if (a.acc != OPS_READ) d->dirty_hd = 2;
     if (d->e_dat && (a.acc == OPS_READ || a.acc == OPS_WRITE || a.acc == OPS_RW))
@@ -1642,6 +1645,16 @@ OPS_API void ops_get_data(ops_dat d) { get_data(d); }
 OPS_API void ops_put_data(ops_dat d) { put_data(d); }
 OPS_API bool ops_checkpointing_init(const char *, double, int) { return false; }
 OPS_API void ops_checkpointing_initphase_done(void) {}
+OPS_API bool ops_checkpointing_before(ops_arg *, int, int *, int) { return true; }
+OPS_API bool ops_checkpointing_name_before(ops_arg *, int, int *, const char *) { return true; }
+OPS_API void ops_checkpointing_manual_datlist(int, ops_dat *) {}
+OPS_API bool ops_checkpointing_fastfw(int, char *) { return false; }
+OPS_API bool ops_checkpointing_manual_datlist_fastfw(int, ops_dat *, int, char *) {
+  return false;
+}
+OPS_API bool ops_checkpointing_manual_datlist_fastfw_trigger(int, ops_dat *, int, char *) {
+  return false;
+}
 OPS_API void ops_reset_gpu_power_counters(void) {}
 OPS_API double ops_get_gpu_energy_consumed(void) { return 0.0; }
 OPS_API void *xmalloc(size_t n) {

@@ -183,6 +183,7 @@ class ConstDecl:
 
 
 ACCESS = {"OPS_READ", "OPS_WRITE", "OPS_RW", "OPS_INC", "OPS_MIN", "OPS_MAX"}
+OB2_MAX_ACC_MACROS = 48  # OPS_ACCn / OPS_ACC_MDn macros given a host meaning
 
 
 def parse_arg(text: str, where: str) -> LoopArg:
@@ -320,6 +321,11 @@ class Translator:
         # strided rows per trip of a reduction kernel's row loop (at least)
         self.rpy = max(1, int(os.environ.get("OPS_B200_RPY", "1")))
         self.light_max = int(os.environ.get("OPS_B200_LIGHT", "4"))
+        # OPS_B200_CHECK=1: OPS_ACCn accesses are checked against their dat's
+        # allocation; an access outside it prints its kernel, argument, point
+        # and offset (device printf) and is redirected to the dat's first
+        # element instead of being made
+        self.check = os.environ.get("OPS_B200_CHECK", "0") == "1"
         self.minb = max(0, int(os.environ.get("OPS_B200_MINB", "4")))
 
     # -- discovery ---------------------------------------------------------
@@ -459,8 +465,14 @@ class Translator:
         out.append(src[last:])
         body = "".join(out)
         protos = "\n".join(self.stub_proto(l) for l in self.loops.values())
-        hdr = ('#include "ops_lib_core.h"\n#include "ops_tridiag.h"\n'
-               "/* generated par_loop stubs (B200 backend) */\n%s\n" % protos)
+        # host code never runs kernel bodies (the stubs launch the device
+        # copies), but it may include kernel headers written with OPS_ACCn
+        # index macros: give them an empty host meaning
+        acc_macros = "".join("#ifndef OPS_ACC%d\n#define OPS_ACC%d(...) 0\n#endif\n"
+                             "#ifndef OPS_ACC_MD%d\n#define OPS_ACC_MD%d(...) 0\n#endif\n" %
+                             (i, i, i, i) for i in range(OB2_MAX_ACC_MACROS))
+        hdr = ('#include "ops_lib_core.h"\n#include "ops_tridiag.h"\n%s'
+               "/* generated par_loop stubs (B200 backend) */\n%s\n" % (acc_macros, protos))
         body, nsub = re.subn(r'^\s*#\s*include\s*[<"]ops_seq(_v2)?\.h[>"].*$', hdr.rstrip("\n"),
                              body, count=1, flags=re.M)
         if nsub == 0:
@@ -502,6 +514,63 @@ class Translator:
         for c in self.consts.values():
             w(self.const_decl(c))
         # all functions of the kernel headers, as device functions
+        # kernels written with pointers and OPS_ACCn(x, y, z) index macros
+        # (the reference's original API) take their dat arguments as
+        # pointers to the point plus, per such argument, the element strides
+        # along x, y, z and between components
+        legacy = {}
+        for loop in self.loops.values():
+            kd = self.kernels.get(loop.kernel)
+            if kd is None or kd.params is None:
+                continue
+            idx = [i for i, (a, p) in enumerate(zip(loop.args, kd.params))
+                   if a.kind == "dat" and not p.is_acc]
+            if idx:
+                legacy[loop.kernel] = (loop.ndim, idx)
+
+        def emit_fn(kd):
+            text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
+            if kd.name not in legacy:
+                if re.search(r"\bOPS_ACC(_MD)?\d+\s*\(", mask_comments_strings(text)):
+                    return  # an OPS_ACCn kernel no loop of this program calls
+                w("static __device__ __forceinline__ " + text)
+                return
+            nd, idx = legacy[kd.name]
+            coords = ["x", "y", "z"][:max(1, min(3, nd))]
+            for i in idx:
+                expr = " + ".join("(%s) * ob2_s%s%d" % (c, c, i) for c in coords)
+                if self.check:
+                    w("#define OPS_ACC%d(%s) ob2_chk(%s, ob2_lo%d, ob2_hi%d, \"%s\", %d)" %
+                      (i, ", ".join(coords), expr, i, i, kd.name, i))
+                    w("#define OPS_ACC_MD%d(d, %s) ob2_chk((d) * ob2_sd%d + %s, ob2_lo%d, ob2_hi%d,"
+                      " \"%s\", %d)" % (i, ", ".join(coords), i, expr, i, i, kd.name, i))
+                    continue
+                w("#define OPS_ACC%d(%s) (%s)" % (i, ", ".join(coords), expr))
+                w("#define OPS_ACC_MD%d(d, %s) ((d) * ob2_sd%d + %s)" %
+                  (i, ", ".join(coords), i, expr))
+            masked = mask_comments_strings(text)
+            op = masked.index("(", masked.find(kd.name))
+            cl = match_paren(masked, op)
+            extra = "".join(", int ob2_sx%d, int ob2_sy%d, int ob2_sz%d, int ob2_sd%d" %
+                            (i, i, i, i) for i in idx)
+            if self.check:
+                extra += "".join(", long long ob2_lo%d, long long ob2_hi%d" % (i, i) for i in idx)
+            w("static __device__ __forceinline__ " + text[:cl] + extra + text[cl:])
+            for i in idx:
+                w("#undef OPS_ACC%d" % i)
+                w("#undef OPS_ACC_MD%d" % i)
+
+        if self.check:
+            w("static __device__ long long ob2_chk(long long m, long long lo, long long hi,"
+              " const char *k, int a) {")
+            w("  if (m >= lo && m < hi) return m;")
+            w("  printf(\"OPS_B200_CHECK: %s arg %d offset %lld outside [%lld, %lld) at thread"
+              " (%d,%d,%d) block (%d,%d,%d)\\n\", k, a, m, lo, hi, (int)threadIdx.x,"
+              " (int)threadIdx.y, (int)threadIdx.z, (int)blockIdx.x, (int)blockIdx.y,"
+              " (int)blockIdx.z);")
+            w("  return lo;")
+            w("}")
+            w("static __device__ double ob2_dummy[64];")
         emitted = set()
         for h in self.headers:
             if not self.is_kernel_header(h):
@@ -510,15 +579,12 @@ class Translator:
                 if kd.name in emitted:
                     continue
                 emitted.add(kd.name)
-                text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
-                w("static __device__ __forceinline__ " + text)
+                emit_fn(kd)
         for loop in self.loops.values():
             if loop.kernel not in self.kernels:
                 raise SystemExit("kernel %s not found in the included headers" % loop.kernel)
             if loop.kernel not in emitted:
-                kd = self.kernels[loop.kernel]
-                text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
-                w("static __device__ __forceinline__ " + text)
+                emit_fn(self.kernels[loop.kernel])
                 emitted.add(loop.kernel)
         for loop in self.loops.values():
             self.emit_loop(loop, w)
@@ -583,11 +649,10 @@ class Translator:
         reds = []
         for i, (a, p) in enumerate(zip(loop.args, kd.params)):
             if a.kind == "dat":
-                if not p.is_acc:
-                    raise SystemExit("kernel %s parameter %d must be an ACC<> for ops_arg_dat" %
-                                     (loop.kernel, i))
                 w("  %s *b%d; long long wx%d, wy%d, wz%d; int ex%d, ey%d, ez%d, ed%d;" %
                   (p.base_type, i, i, i, i, i, i, i, i))
+                if self.check:
+                    w("  long long clo%d, chi%d;" % (i, i))
             elif a.kind == "gbl":
                 w("  %s g%d[%s];" % (p.base_type, i, a.dim))
             elif a.kind == "reduce":
@@ -617,8 +682,13 @@ class Translator:
                     # only optional arguments can carry a null dat
                     ptr = ("q%d ? q%d + %s : (%s *)0" % (i, i, off, p.base_type)) if a.opt \
                         else "q%d + %s" % (i, off)
-                    w("  ACC<%s> a%d(%s, %s, p.ey%d, p.ez%d, p.ed%d);" %
-                      (p.base_type, i, ptr, ex, i, i, i))
+                    if p.is_acc:
+                        w("  ACC<%s> a%d(%s, %s, p.ey%d, p.ez%d, p.ed%d);" %
+                          (p.base_type, i, ptr, ex, i, i, i))
+                    else:  # OPS_ACCn kernel: the point's pointer (strides below)
+                        if self.check and a.opt:  # a disabled argument points at a dummy
+                            ptr = "q%d ? q%d + %s : (%s *)ob2_dummy" % (i, i, off, p.base_type)
+                        w("  %s *a%d = %s;" % (p.base_type, i, ptr))
                     call.append("a%d" % i)
                 elif a.kind == "gbl":
                     call.append("(%s *)p.g%d" % (p.base_type, i))
@@ -628,6 +698,15 @@ class Translator:
                     call.append("idx")
             if any(a.kind == "idx" for a in loop.args):
                 w("  int idx[3] = {x, y, z};")
+            for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+                if a.kind == "dat" and not p.is_acc:
+                    ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
+                    call.append("%s, p.ey%d, p.ez%d, p.ed%d" % (ex, i, i, i))
+            if self.check:
+                for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+                    if a.kind == "dat" and not p.is_acc:
+                        po = "(x * p.wx%d + y * p.wy%d + z * p.wz%d)" % (i, i, i)
+                        call.append("p.clo%d - %s, p.chi%d - %s" % (i, po, i, po))
             w("  %s(%s);" % (loop.kernel, ", ".join(call)))
             w("}")
         w("template <bool RESTRICT, bool IDX32>")
@@ -794,6 +873,13 @@ class Translator:
                   " p.wz%d = L.view[%d].wz;" % (i, p.base_type, i, i, i, i, i, i, i))
                 w("  p.ex%d = L.view[%d].ex; p.ey%d = L.view[%d].ey; p.ez%d = L.view[%d].ez;"
                   " p.ed%d = L.view[%d].ed;" % (i, i, i, i, i, i, i, i))
+                if self.check:
+                    w("  if (arg%d.dat && L.view[%d].base) {" % (i, i))
+                    w("    p.clo%d = (long long)((char *)arg%d.dat->data_d - L.view[%d].base) /"
+                      " (long long)sizeof(%s);" % (i, i, i, p.base_type))
+                    w("    p.chi%d = p.clo%d + (long long)(arg%d.dat->mem / sizeof(%s));" %
+                      (i, i, i, p.base_type))
+                    w("  } else { p.clo%d = 0; p.chi%d = 0; }" % (i, i))
             elif a.kind == "gbl":
                 w("  if ((size_t)arg%d.dim * (size_t)arg%d.elem_size > sizeof(p.g%d))"
                   " throw OPSException(OPS_INVALID_ARGUMENT, \"Error: ops_arg_gbl larger than"

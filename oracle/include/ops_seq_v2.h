@@ -57,7 +57,9 @@ template <typename P> struct holder {
 template <typename T> struct acc_holder {
   ACC<T> a;
   void set(const ops_arg &arg, const int *, const int *pt, ops_block block) {
-    if (arg.argtype != OPS_ARG_DAT || !arg.opt || arg.dat == NULL) {
+    // a disabled optional argument still points at its dat, as in the
+    // reference's sequential backend (the flag only matters to halo exchanges)
+    if (arg.argtype != OPS_ARG_DAT || arg.dat == NULL) {
       a = ACC<T>();
       return;
     }

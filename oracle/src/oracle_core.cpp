@@ -571,6 +571,16 @@ OPS_API void ops_get_data(ops_dat) {}
 OPS_API void ops_put_data(ops_dat) {}
 OPS_API bool ops_checkpointing_init(const char *, double, int) { return false; }
 OPS_API void ops_checkpointing_initphase_done(void) {}
+OPS_API bool ops_checkpointing_before(ops_arg *, int, int *, int) { return true; }
+OPS_API bool ops_checkpointing_name_before(ops_arg *, int, int *, const char *) { return true; }
+OPS_API void ops_checkpointing_manual_datlist(int, ops_dat *) {}
+OPS_API bool ops_checkpointing_fastfw(int, char *) { return false; }
+OPS_API bool ops_checkpointing_manual_datlist_fastfw(int, ops_dat *, int, char *) {
+  return false;
+}
+OPS_API bool ops_checkpointing_manual_datlist_fastfw_trigger(int, ops_dat *, int, char *) {
+  return false;
+}
 OPS_API void ops_reset_gpu_power_counters(void) {}
 OPS_API double ops_get_gpu_energy_consumed(void) { return 0.0; }
 

@@ -94,3 +94,34 @@ def clover_deck_test2() -> str:
             "ymax=2.0\n x_cells=960\n y_cells=960\n xmin=0.0\n ymin=0.0\n xmax=10.0\n ymax=10.0\n"
             " initial_timestep=0.04\n timestep_rise=1.5\n max_timestep=0.04\n end_step=87\n"
             " test_problem 2\n*endclover\n")
+
+
+def clover3d_deck_test2() -> str:
+    """CloverLeaf 3D test problem 2 (CloverLeaf_3D/field_summary.cpp:95,
+    expected kinetic energy 20.0546870878964): 96^3 cells on a 10^3 domain, a
+    dense cuboid [0,5] x [0,2] x [0,4], 87 steps.  checkpoint_frequency must be
+    set: the app takes `step % checkpoint_frequency` every step
+    (CloverLeaf_3D/clover_leaf.cpp:209) and gives it no default."""
+    return ("*clover\n state 1 density=0.2 energy=1.0\n"
+            " state 2 density=1.0 energy=2.5 geometry=cuboid xmin=0.0 xmax=5.0 ymin=0.0 "
+            "ymax=2.0 zmin=0.0 zmax=4.0\n x_cells=96\n y_cells=96\n z_cells=96\n"
+            " xmin=0.0\n ymin=0.0\n zmin=0.0\n xmax=10.0\n ymax=10.0\n zmax=10.0\n"
+            " initial_timestep=0.1\n max_timestep=0.1\n end_step=87\n end_time=1000.1\n"
+            " test_problem 2\n checkpoint_frequency=10\n*endclover\n")
+
+
+def tealeaf_deck_test1(solver: str = "tl_use_jacobi") -> str:
+    """TeaLeaf test problem 1 (TeaLeaf/field_summary.cpp:84, expected
+    temperature 157.55084183279294): 10 x 10 cells on a 10 x 10 domain, four
+    low-density strips over a dense background, 10 steps, solver tolerance
+    1e-15 (the reference's default deck uses Jacobi; CG and Chebyshev reach the
+    same solution)."""
+    states = [" state 1 density=100.0 energy=0.0001"]
+    for k, (e, x0, x1, y0, y1) in enumerate([(25.0, 0, 1, 1, 2), (0.1, 1, 6, 1, 2),
+                                              (0.1, 5, 6, 1, 8), (0.1, 5, 10, 7, 8)]):
+        states.append(" state %d density=0.1 energy=%s geometry=rectangle xmin=%.1f xmax=%.1f "
+                      "ymin=%.1f ymax=%.1f" % (k + 2, e, x0, x1, y0, y1))
+    return ("*tea\n" + "\n".join(states) +
+            "\n x_cells=10\n y_cells=10\n xmin=0.0\n ymin=0.0\n xmax=10.0\n ymax=10.0\n"
+            " initial_timestep=0.004\n end_step=10\n tl_max_iters=1000\n %s\n tl_eps=1e-15\n"
+            " test_problem 1\n*endtea\n" % solver)

@@ -228,3 +228,27 @@ def test_more_reference_apps_match_oracle(tmp_path, name, args, mode, text):
         check_dumps(dumps["b200"], dumps["oracle"], tol=1e-12, float_tol=1e-6, floor_frac=1.0)
     elif mode == "libm":
         check_dumps(dumps["b200"], dumps["oracle"], tol=1e-6, float_tol=1e-5, floor_frac=1.0)
+
+
+@pytest.mark.parametrize("solver", ["tl_use_jacobi", "tl_use_cg", "tl_use_chebyshev"])
+def test_reference_tealeaf_known_answer_on_b200(solver):
+    """TeaLeaf, written with the original OPS_ACCn kernel API, built unchanged:
+    test problem 1 passes the reference's own check (within 0.001 % of the
+    expected temperature)."""
+    from tests.apprun import tealeaf_deck_test1
+    d = tempfile.mkdtemp(prefix="tea_")
+    with open(os.path.join(d, "tea.in"), "w") as f:
+        f.write(tealeaf_deck_test1(solver))
+    out = run_exe("ref_tealeaf", "b200", cwd=d)
+    assert "This test is considered PASSED" in out, out[-1500:]
+
+
+def test_reference_cloverleaf3d_known_answer_on_b200():
+    """CloverLeaf 3D (original OPS_ACCn kernel API) built unchanged: test
+    problem 2, 96^3 cells, 87 steps, passes the reference's own check."""
+    from tests.apprun import clover3d_deck_test2
+    d = tempfile.mkdtemp(prefix="clover3d_")
+    with open(os.path.join(d, "clover.in"), "w") as f:
+        f.write(clover3d_deck_test2())
+    out = run_exe("ref_cloverleaf3d", "b200", cwd=d)
+    assert "This test is considered PASSED" in out, out[-1500:]
