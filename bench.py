@@ -241,7 +241,9 @@ def run_ours(a, d: Dist):
     d.barrier()
     clocks.start()
     B.ob2_event_record(ev0)
+    h0 = time.perf_counter()
     L.clover_step_run(a.steps)
+    host_s = time.perf_counter() - h0  # host time to issue the K steps
     B.ob2_event_record(ev1)
     ms = ctypes.c_float()
     rc = B.ob2_event_elapsed_ms(ev0, ev1, ctypes.byref(ms))
@@ -254,6 +256,13 @@ def run_ours(a, d: Dist):
     # around every launch, kept out of the timed region above (recording
     # ~300 events per step adds host work to every step)
     report = ""
+    if a.report:  # lazy-queue statistics (chains, graph replays and updates)
+        B.ops_timing_output_str.restype = ctypes.c_size_t
+        n = B.ops_timing_output_str(None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        B.ops_timing_output_str(buf, n + 1)
+        sys.stderr.write("timed steps: host issue %.3f ms/step, device %.3f ms/step\n%s\n" %
+                         (host_s * 1e3 / a.steps, ms.value / a.steps, buf.value.decode()))
     if a.ktime:
         B.ob2_ktime_reset()
         B.ob2_ktime_enable(1)

@@ -267,14 +267,18 @@ def main(argv=None) -> int:
     ap.add_argument("--inner-tol", type=float, default=1e-2,
                     help="residual drop between FP64 residual replacements")
     ap.add_argument("--seed", type=int, default=6)
-    ap.add_argument("--max-n", type=int, default=2048)
+    ap.add_argument("--min-n", type=int, default=64, help="smallest Poisson grid")
+    ap.add_argument("--max-n", type=int, default=2048, help="largest Poisson grid")
+    ap.add_argument("--adi-frac", type=float, default=0.3, help="share of ADI requests")
     a = ap.parse_args(argv)
-    stream_args = dict(count=a.requests, rate=a.rate, seed=a.seed, pois_n=(64, a.max_n))
+    stream_args = dict(count=a.requests, rate=a.rate, seed=a.seed, pois_n=(a.min_n, a.max_n),
+                       adi_frac=a.adi_frac)
     budget = int(a.budget_gb * 1e9)
     out = {"config": {"requests": a.requests, "rate": a.rate, "budget_gb": a.budget_gb,
                       "iters_per_replay": a.iters, "tile_y": a.tile_y,
                       "inner_tol": a.inner_tol, "seed": a.seed, "tol": 1e-8,
-                      "poisson_n": [64, a.max_n], "adi_n": [32, 192], "adi_steps": 10}}
+                      "poisson_n": [a.min_n, a.max_n], "adi_frac": a.adi_frac,
+                      "adi_n": [32, 192], "adi_steps": 10}}
     sols = {}
     if a.mode in ("mixed", "both"):
         e = Engine(MIXED, inner_tol=a.inner_tol, tile_y=a.tile_y)
