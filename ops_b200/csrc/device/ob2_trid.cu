@@ -246,20 +246,28 @@ __global__ void __launch_bounds__(kThreads) trid_staged_kernel(
   }
 }
 
-// Long lines (n > 32*16): LPB lines per CTA, P chunks per line spread over
-// the CTA, PCR over the 2P end unknowns in shared memory.
-template <typename T, bool INC, int CL>
+// LPB lines per CTA, P chunks per line spread over the CTA, PCR over the 2P
+// end unknowns in shared memory.  Chunk-major mapping (LM false: the P
+// chunks of a line on consecutive threads) for long lines (n > 32*16);
+// line-major mapping (LM true: consecutive threads on the same chunk of
+// neighbouring lines) for strided lines, whose neighbours along the fastest
+// other axis are contiguous in memory, so that every load and store of a
+// warp is two runs of LPB elements and no scratch is needed.  The
+// arithmetic of a line does not depend on the mapping.
+template <typename T, bool INC, int CL, bool LM>
 __global__ void __launch_bounds__(kThreads) trid_cta_kernel(
     int n, int P, int LPB, long long nlines, long long stride, int o1n, long long o1s,
     long long o2s, const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
     T *__restrict__ D, T *__restrict__ U) {
   extern __shared__ double sm[];
   const int tid = threadIdx.x;
-  const int p = tid % P, l = tid / P;
+  const int p = LM ? tid / LPB : tid % P, l = LM ? tid % LPB : tid / P;
   const long long line = (long long)blockIdx.x * LPB + l;
   const bool active = line < nlines && l < LPB;
   const int m = 2 * P;
-  double *ra = sm + (size_t)(l < LPB ? l : 0) * m * 3;
+  // a line's 3 x 2P values; the odd pitch spreads neighbouring lines over
+  // the shared-memory banks
+  double *ra = sm + (size_t)(l < LPB ? l : 0) * (m * 3 + 1);
   double *rc = ra + m;
   double *rd = rc + m;
   long long base = 0;
@@ -465,38 +473,56 @@ int launch_staged(const Lines &g, const void *a, const void *b, const void *c, v
   return (int)cudaGetLastError();
 }
 
-template <typename T, int CL>
+template <typename T, int CL, bool LM>
 int launch_cta(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
   const int P = (g.n + CL - 1) / CL;
   if (P > kThreads) return (int)cudaErrorInvalidValue;
   const int LPB = kThreads / P;
   const int threads = LPB * P;
-  const size_t shmem = (size_t)LPB * 2 * P * 3 * sizeof(double);
+  const size_t shmem = (size_t)LPB * (2 * P * 3 + 1) * sizeof(double);
   const long long grid = (g.nlines + LPB - 1) / LPB;
   if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
   cudaStream_t st = (cudaStream_t)ob2_dev_stream();
   if (u)
-    trid_cta_kernel<T, true, CL><<<(unsigned)grid, threads, shmem, st>>>(
+    trid_cta_kernel<T, true, CL, LM><<<(unsigned)grid, threads, shmem, st>>>(
         g.n, P, LPB, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
         (const T *)c, (T *)d, (T *)u);
   else
-    trid_cta_kernel<T, false, CL><<<(unsigned)grid, threads, shmem, st>>>(
+    trid_cta_kernel<T, false, CL, LM><<<(unsigned)grid, threads, shmem, st>>>(
         g.n, P, LPB, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a, (const T *)b,
         (const T *)c, (T *)d, (T *)nullptr);
   return (int)cudaGetLastError();
 }
 
-// OB2_TRID_STRIDED: how strided lines are solved: 1 the staged warp-per-line
-// kernel (default; 296 / 410 us for the 256^3 y / z solves), 0 the Thomas
-// kernel (bit-identical to the sequential restatement; 365 / 409 us: its
-// c'/d' scratch traffic and division chain cost more than the PCR)
-bool use_thomas(int unit) {
-  static int v = -1;
-  if (v < 0) {
+// OB2_TRID_STRIDED: how strided lines are solved.  Measured on the 256^3
+// FP64 y / z solves (CUDA events, 20 steps): 3 the line-major CTA kernel
+// with 8-point chunks (8 lines x 32 chunks per CTA, 64-byte runs, 2 CTAs per
+// SM): 226 / 364 us; 2 the same with 16-point chunks (16 lines, 128-byte
+// runs, 150 registers, 1 CTA per SM): 213 / 438 us; 1 the staged
+// warp-per-line kernel: 300 / 408 us; 0 the Thomas kernel (bit-identical to
+// the sequential restatement): 371 / 382 us.  With FP32 storage the
+// line-major runs shrink to 32 bytes and the staged kernel is faster
+// (290 / 400 us against 305 / 428 us).  Default (-1): 3 for 8-byte values
+// and lines of up to 256 points, 1 otherwise.
+int strided_mode() {
+  static int v = -2;
+  if (v == -2) {
     const char *e = getenv("OB2_TRID_STRIDED");
-    v = e ? atoi(e) : 1;
+    v = e ? atoi(e) : -1;
   }
-  return !unit && v == 0;
+  return v;
+}
+bool use_thomas(int unit) { return !unit && strided_mode() == 0; }
+
+// the line-major CTA kernel's chunk length for strided lines, 0: not used
+template <typename T>
+int line_major_chunk(const Lines &g) {
+  if (g.unit) return 0;
+  const int m = strided_mode();
+  if (m == 2 && g.n <= 32 * 16) return 16;
+  if (m == 3 && g.n <= 32 * 8) return 8;
+  if (m == -1 && sizeof(T) == 8 && g.n <= 32 * 8) return 8;
+  return 0;
 }
 
 // OB2_TRID_STAGED: 0 never, 1 always, 2 strided lines only (default)
@@ -529,6 +555,14 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   g.unit = g.stride == 1 ? 1 : 0;
   if (g.n <= 0 || g.nlines <= 0) return 0;
   if (use_thomas(g.unit)) return launch_thomas<T>(g, a, b, c, d, u);
+  switch (line_major_chunk<T>(g)) {
+    case 8:
+      return launch_cta<T, 8, true>(g, a, b, c, d, u);
+    case 16:
+      return launch_cta<T, 16, true>(g, a, b, c, d, u);
+    default:
+      break;
+  }
   if (g.n <= 32 * 16) {
     const bool st = use_staged(g.unit);
     if (g.n <= 32 * 4)
@@ -537,7 +571,7 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
       return st ? launch_staged<T, 8>(g, a, b, c, d, u) : launch_warp<T, 8>(g, a, b, c, d, u);
     return st ? launch_staged<T, 16>(g, a, b, c, d, u) : launch_warp<T, 16>(g, a, b, c, d, u);
   }
-  return launch_cta<T, 16>(g, a, b, c, d, u);
+  return launch_cta<T, 16, false>(g, a, b, c, d, u);
 }
 
 }  // namespace

@@ -182,3 +182,23 @@ def test_trid_thomas_strided_bit_exact(typ, solvedim, inc):
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                        env=dict(os.environ, OB2_TRID_STRIDED="0"), timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("mode", ["1", "2", "3"])
+@pytest.mark.parametrize("typ", ["double", "float"])
+def test_trid_strided_kernels(mode, typ):
+    """Every kernel for strided lines -- OB2_TRID_STRIDED=1 the staged
+    warp-per-line kernel, 2 and 3 the line-major CTA kernel with 16- and
+    8-point chunks -- against the numpy Thomas model: y and z lines, with and
+    without _Inc, line counts that do not fill the last CTA, line lengths
+    from 5 to 200 (a child process per mode: the choice is read once)."""
+    import subprocess
+    import sys
+    calls = "; ".join("t.test_trid_batch(%r, %d, %r, %r)" % (typ, sd, inc, shape)
+                      for sd in (1, 2) for inc in (False, True)
+                      for shape in ((9, 37, 11), (19, 5, 200), (33, 7, 5)))
+    code = ("import sys; sys.path.insert(0, %r); import tests.test_gpu_cabi as t; %s" %
+            (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), calls))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       env=dict(os.environ, OB2_TRID_STRIDED=mode), timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
