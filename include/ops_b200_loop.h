@@ -33,6 +33,19 @@ typedef struct ob2_red {
   int op;       /* OPS_INC / OPS_MIN / OPS_MAX */
 } ob2_red;
 
+/* A generated fused launcher (one per application): runs n (<= OB2_FUSE_MAX)
+ * different loops of the application in one launch, loop k being the
+ * application's loop ids[k] with parameter block params[k] (psize[k] bytes,
+ * each rounded up to 16, together at most OB2_FUSE_BLOB) over its own grid
+ * grids[3k..3k+2]; every loop takes the CTA shape `block`.  idx32: every
+ * loop has 32-bit element offsets.  The runtime only passes loops that touch
+ * no common point of a dat that one of them writes. */
+#define OB2_FUSE_MAX 16
+#define OB2_FUSE_BLOB 8192
+typedef int (*ob2_flauncher)(int n, const int *ids, const void *const *params,
+                             const size_t *psize, const unsigned *grids, const unsigned *block,
+                             int idx32, void *stream);
+
 typedef struct ob2_loop {
   const char *name;
   int kernel_index;  /* timing-table slot */
@@ -58,6 +71,9 @@ typedef struct ob2_loop {
                                offsets fit 32-bit arithmetic */
   int tune;                 /* >= 0: this launch times block-shape candidate
                                `tune` of the autotuner (OPS_B200_AUTOTUNE) */
+  int fuse_id;              /* the loop's id in the fused launcher, -1: none */
+  ob2_flauncher ffn;        /* the application's fused launcher (set by the
+                               stub before ob2_launch; NULL: none) */
 } ob2_loop;
 
 /* A generated launcher: launches one kernel variant with the parameter block
@@ -84,9 +100,14 @@ typedef int (*ob2_mlauncher)(const void *const *params, int n, const unsigned *g
  * OPS_CACHE_SIZE (MB), the GPU form of the reference's loop-chain tiling,
  * ops_lazy.cpp:380-1187.  Consecutive queued instances of one loop with
  * no data shared between them (the blocks of a multi-block program) run as
- * one launch of mfn (may be NULL: loops with reductions).  rows_per_thread:
- * points each thread covers along y (the grid's y extent is derived from it
- * per tile). */
+ * one launch of mfn (may be NULL: loops with reductions).  Consecutive
+ * queued small loops (up to OPS_B200_FUSE_PTS points each, default 65536)
+ * that share no point of a dat that one of them writes -- each loop writes
+ * its range and reads its range shifted by every stencil point -- run as one
+ * launch of the application's fused launcher L->ffn (OPS_B200_FUSE=0: off);
+ * the boundary loops of a halo update are the typical case.
+ * rows_per_thread: points each thread covers along y (the grid's y extent
+ * is derived from it per tile). */
 OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const void *params,
                         size_t psize, const unsigned *grid, const unsigned *block,
                         int rows_per_thread);

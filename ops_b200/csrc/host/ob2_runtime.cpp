@@ -117,11 +117,18 @@ struct Runtime {
   std::string tune_file;      // decisions read at ops_init, written at ops_exit
   std::unordered_map<std::string, std::array<int, 3>> tune_known;
   double cache_mb = 40.0;   // L2 budget per tile (OPS_CACHE_SIZE, MB)
-  struct QAcc { int dat; int acc; int rmin, rmax; int flat; };  // no padding: hashed as bytes
+  // sx: the stencil's stride per axis (0: the axis of an edge dat, indexed
+  // by the stencil offset alone); any: other strides or long stencils (taken
+  // to touch everything); sidx: the stencil (index into Runtime::stencils,
+  // -1: none)
+  struct QAcc { int dat; int acc; int rmin, rmax; int flat; int sx[3]; int any; int sidx; };  // no padding: hashed as bytes
   struct QItem {
     int kind;               // 0 par_loop, 1 halo group
     ob2_launcher fn;
     ob2_mlauncher mfn;      // multi-instance launcher (NULL: none)
+    ob2_flauncher ffn;      // the application's fused launcher (NULL: none)
+    int fid, idx32;         // id in ffn; 32-bit offsets
+    long long npts;         // points of the range
     std::vector<char> prm;
     unsigned grid[3], block[3];
     int py, ndim, kidx;
@@ -138,6 +145,9 @@ struct Runtime {
   std::unordered_map<std::string, Graph> graph_cache;  // key: the chain's shape
   long long chains = 0, graph_hits = 0, graph_updates = 0, tiles_run = 0, multi_launches = 0;
   bool multi = true;          // run independent instances of a loop in one launch
+  bool fuse = true;           // run independent small loops in one launch
+  long long fuse_pts = 65536; // largest loop (points) that is fused
+  long long fused_launches = 0, fused_loops = 0;
 };
 
 Runtime *R = nullptr;
@@ -482,6 +492,99 @@ void run_multi(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
   kt_end(ev, q[i].kidx);
 }
 
+// the points of a dat that loop A touches through access x at stencil
+// offset pa and loop B through y at pb intersect (per axis: the loop range
+// shifted by the offset, or the offset alone on a stride-0 axis)
+bool boxes_meet(const Runtime::QItem &A, const Runtime::QAcc &x, const int *pa,
+                const Runtime::QItem &B, const Runtime::QAcc &y, const int *pb) {
+  for (int k = 0; k < 3; k++) {
+    const int alo = x.sx[k] ? A.lo[k] + pa[k] : pa[k], ahi = x.sx[k] ? A.hi[k] + pa[k] : pa[k] + 1;
+    const int blo = y.sx[k] ? B.lo[k] + pb[k] : pb[k], bhi = y.sx[k] ? B.hi[k] + pb[k] : pb[k] + 1;
+    if (ahi <= blo || bhi <= alo) return false;
+  }
+  return true;
+}
+
+// loop A writes (at the centre point, the only point an OPS kernel may
+// write) a point of the dat that loop B touches at its centre or at one of
+// its stencil points
+bool writes_into(const Runtime::QItem &A, const Runtime::QAcc &x, const Runtime::QItem &B,
+                 const Runtime::QAcc &y) {
+  static const int zero[3] = {0, 0, 0};
+  if (boxes_meet(A, x, zero, B, y, zero)) return true;
+  if (y.sidx < 0) return false;
+  const ops_stencil_core *st = rt().stencils[y.sidx];
+  for (int p = 0; p < st->points; p++) {
+    int o[3] = {0, 0, 0};
+    for (int k = 0; k < 3 && k < st->dims; k++) o[k] = st->stencil[p * st->dims + k];
+    if (boxes_meet(A, x, zero, B, y, o)) return true;
+  }
+  return false;
+}
+
+// two queued loops touch a common point of a dat that one of them writes
+bool footprint_conflict(const Runtime::QItem &a, const Runtime::QItem &b) {
+  for (auto &x : a.acc)
+    for (auto &y : b.acc) {
+      if (x.dat != y.dat || (x.acc == OPS_READ && y.acc == OPS_READ)) continue;
+      if (x.any || y.any) return true;
+      if (x.acc != OPS_READ && writes_into(a, x, b, y)) return true;
+      if (y.acc != OPS_READ && writes_into(b, y, a, x)) return true;
+    }
+  return false;
+}
+
+bool fusable(const Runtime::QItem &a) {
+  const Runtime &r = rt();
+  return r.fuse && !r.ktime && a.kind == 0 && a.ffn && a.fid >= 0 && a.npts <= r.fuse_pts &&
+         a.prm.size() <= OB2_FUSE_BLOB;
+}
+
+// q[i] starts a run of small loops that can share one fused launch: returns
+// the end of the run (at most OB2_FUSE_MAX loops, parameter blocks within
+// OB2_FUSE_BLOB, one CTA shape, no footprint conflict between any two)
+size_t fuse_run(const std::vector<Runtime::QItem> &q, size_t i) {
+  const Runtime::QItem &a = q[i];
+  if (!fusable(a)) return i + 1;
+  size_t bytes = (a.prm.size() + 15) & ~(size_t)15;
+  size_t j = i + 1;
+  while (j < q.size() && j - i < OB2_FUSE_MAX) {
+    const Runtime::QItem &b = q[j];
+    if (!fusable(b) || b.ffn != a.ffn || b.idx32 != a.idx32 || b.block[0] != a.block[0] ||
+        b.block[1] != a.block[1] || b.block[2] != a.block[2])
+      break;
+    const size_t nb = (b.prm.size() + 15) & ~(size_t)15;
+    if (bytes + nb > OB2_FUSE_BLOB) break;
+    bool ok = true;
+    for (size_t k = i; k < j && ok; k++) ok = !footprint_conflict(q[k], b);
+    if (!ok) break;
+    bytes += nb;
+    j++;
+  }
+  return j;
+}
+
+void run_fused(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
+  Runtime &r = rt();
+  const int n = (int)(j - i);
+  int ids[OB2_FUSE_MAX];
+  const void *prm[OB2_FUSE_MAX];
+  size_t psz[OB2_FUSE_MAX];
+  unsigned grids[3 * OB2_FUSE_MAX];
+  for (int k = 0; k < n; k++) {
+    const Runtime::QItem &it = q[i + k];
+    ids[k] = it.fid;
+    prm[k] = it.prm.data();
+    psz[k] = it.prm.size();
+    for (int d = 0; d < 3; d++) grids[3 * k + d] = it.grid[d];
+  }
+  check(q[i].ffn(n, ids, prm, psz, grids, q[i].block, q[i].idx32, ob2_dev_stream()),
+        "ops_par_loop launch (fused)");
+  r.launches++;
+  r.fused_launches++;
+  r.fused_loops += n;
+}
+
 void run_queue(std::vector<Runtime::QItem> &q) {
   Runtime &r = rt();
   size_t i = 0;
@@ -496,9 +599,15 @@ void run_queue(std::vector<Runtime::QItem> &q) {
       }
     }
     if (q[i].kind == 0) {
-      const size_t j = multi_run(q, i);
+      size_t j = multi_run(q, i);
       if (j - i >= 2) {
         run_multi(q, i, j);
+        i = j;
+        continue;
+      }
+      j = fuse_run(q, i);
+      if (j - i >= 2) {
+        run_fused(q, i, j);
         i = j;
         continue;
       }
@@ -537,6 +646,8 @@ OPS_API void ob2_flush(void) {
     put(&it.kind, sizeof it.kind);
     put(&it.fn, sizeof it.fn);
     put(&it.mfn, sizeof it.mfn);
+    put(&it.ffn, sizeof it.ffn);
+    put(&it.fid, sizeof it.fid);
     const size_t np = it.prm.size();
     put(&np, sizeof np);
     put(it.grid, sizeof it.grid);
@@ -625,6 +736,10 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
   it.kind = 0;
   it.fn = fn;
   it.mfn = mfn;
+  it.ffn = L->ffn;
+  it.fid = L->fuse_id;
+  it.idx32 = L->idx32;
+  it.npts = L->npoints;
   it.prm.assign((const char *)params, (const char *)params + psize);
   for (int i = 0; i < 3; i++) {
     it.grid[i] = grid[i];
@@ -653,6 +768,15 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
         qa.rmin = std::min(qa.rmin, o);
         qa.rmax = std::max(qa.rmax, o);
       }
+    // for the footprint test of fused launches: the stencil and its strides
+    qa.any = 0;
+    qa.sidx = a.stencil ? a.stencil->index : -1;
+    for (int k = 0; k < 3; k++) {
+      const int st = a.stencil ? a.stencil->stride[k] : 1;
+      qa.sx[k] = st;
+      if (st != 0 && st != 1) qa.any = 1;
+    }
+    if (a.stencil && a.stencil->points > 32) qa.any = 1;  // keeps the test short
     it.acc.push_back(qa);
   }
   r.q.push_back(std::move(it));
@@ -696,6 +820,8 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_RED_WAVES"))) r.red_waves = std::max(1, atoi(e));
   if ((e = getenv("OPS_B200_AUTOTUNE"))) r.autotune = atoi(e) != 0;
   if ((e = getenv("OPS_B200_MULTI"))) r.multi = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_FUSE"))) r.fuse = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_FUSE_PTS"))) r.fuse_pts = atoll(e);
   if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
     r.tune_file = e;
     if (FILE *f = fopen(e, "r")) {  // decisions of an earlier run
@@ -1297,6 +1423,8 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->block[2] = dim > 2 ? r.block_z : 1;
   L->host_t0 = wall();
   L->ev_start = L->ev_end = nullptr;
+  L->fuse_id = -1;  // the stub names its fused launcher after this call
+  L->ffn = nullptr;
   if (L->npoints == 0) return 0;
 
   size_t red_bytes = 0;
@@ -1581,8 +1709,10 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
   if (r.lazy) {
     snprintf(line, sizeof line,
              "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "
-             "%lld tile launches, %lld multi-instance launches\n",
-             r.chains, r.graph_hits, r.graph_updates, r.tiles_run, r.multi_launches);
+             "%lld tile launches, %lld multi-instance launches, %lld fused launches "
+             "(%lld loops)\n",
+             r.chains, r.graph_hits, r.graph_updates, r.tiles_run, r.multi_launches,
+             r.fused_launches, r.fused_loops);
     s += line;
   }
   if (buf && n) {

@@ -511,6 +511,11 @@ class Translator:
             w('#include "%s"' % h)
         w("#define OB2_CONST_CAP(T) ((4096 + sizeof(T) - 1) / sizeof(T))")
         w("namespace ob2_%s {" % re.sub(r"\W", "_", self.app))
+        # the application's fused launcher (defined after all loops)
+        w("static int ob2f_launch(int n, const int *ids, const void *const *prm,"
+          " const size_t *psz, const unsigned *grids, const unsigned *block, int idx32,"
+          " void *st);")
+        self.fuse_items = []
         for c in self.consts.values():
             w(self.const_decl(c))
         # all functions of the kernel headers, as device functions
@@ -588,6 +593,7 @@ class Translator:
                 emitted.add(loop.kernel)
         for loop in self.loops.values():
             self.emit_loop(loop, w)
+        self.emit_fused(w)
         # constant copier
         w("static int ob2_const_copy(const char *name, int dim, int type_size, const char *data,"
           " void *stream) {")
@@ -607,6 +613,67 @@ class Translator:
         w("}  // namespace")
         with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
             f.write("\n".join(L) + "\n")
+
+    def emit_fused(self, w) -> None:
+        """One kernel that runs several different loops of the application
+        in one launch (the runtime passes only loops whose footprints do not
+        meet): loop k of the launch takes CTAs [cta0[k], cta0[k+1]) and runs
+        the body of loop id[k] on its own parameter block and grid, through
+        the body's unrestricted variant."""
+        items = self.fuse_items
+        w("struct ob2_fuse_params {")
+        w("  int n;")
+        w("  unsigned cta0[OB2_FUSE_MAX + 1], gx[OB2_FUSE_MAX], gy[OB2_FUSE_MAX];")
+        w("  int id[OB2_FUSE_MAX];")
+        w("  unsigned off[OB2_FUSE_MAX];")
+        w("  alignas(16) char blob[OB2_FUSE_BLOB];")
+        w("};")
+        lb = "512, %d" % self.minb if self.minb > 0 else "512"
+        w("template <bool IDX32>")
+        w("__global__ void __launch_bounds__(%s) ob2fk(const __grid_constant__ ob2_fuse_params f) {"
+          % lb)
+        w("  const unsigned b = blockIdx.x;")
+        w("  int i = 0;")
+        w("  while (i + 1 < f.n && b >= f.cta0[i + 1]) i++;")
+        w("  const unsigned loc = b - f.cta0[i], r = loc / f.gx[i];")
+        w("  const unsigned bx = loc - r * f.gx[i], by = r % f.gy[i], bz = r / f.gy[i];")
+        w("  const char *prm = f.blob + f.off[i];")
+        w("  switch (f.id[i]) {")
+        for k, (P, BF) in enumerate(items):
+            w("    case %d: %s<false, IDX32>(*(const %s *)prm, bx, by, bz); break;" % (k, BF, P))
+        w("    default: break;")
+        w("  }")
+        w("}")
+        w("static int ob2f_launch(int n, const int *ids, const void *const *prm,"
+          " const size_t *psz, const unsigned *grids, const unsigned *block, int idx32,"
+          " void *st) {")
+        w("  if (n < 1 || n > OB2_FUSE_MAX) return (int)cudaErrorInvalidValue;")
+        w("  static ob2_fuse_params f;  // host staging (one host thread drives OPS)")
+        w("  f.n = n;")
+        w("  unsigned long long c = 0;")
+        w("  size_t off = 0;")
+        w("  for (int k = 0; k < n; k++) {")
+        w("    if (ids[k] < 0 || ids[k] >= %d) return (int)cudaErrorInvalidValue;" % len(items))
+        w("    off = (off + 15) & ~(size_t)15;")
+        w("    if (off + psz[k] > OB2_FUSE_BLOB) return (int)cudaErrorInvalidValue;")
+        w("    memcpy(f.blob + off, prm[k], psz[k]);")
+        w("    f.off[k] = (unsigned)off;")
+        w("    off += psz[k];")
+        w("    f.id[k] = ids[k];")
+        w("    f.cta0[k] = (unsigned)c;")
+        w("    f.gx[k] = grids[3 * k];")
+        w("    f.gy[k] = grids[3 * k + 1];")
+        w("    c += (unsigned long long)grids[3 * k] * grids[3 * k + 1] * grids[3 * k + 2];")
+        w("  }")
+        w("  if (c == 0 || c > 0x7fffffffULL) return (int)cudaErrorInvalidValue;")
+        w("  f.cta0[n] = (unsigned)c;")
+        w("  const dim3 blk(block[0], block[1], block[2]);")
+        w("  if (idx32)")
+        w("    ob2fk<true><<<(unsigned)c, blk, 0, (cudaStream_t)st>>>(f);")
+        w("  else")
+        w("    ob2fk<false><<<(unsigned)c, blk, 0, (cudaStream_t)st>>>(f);")
+        w("  return (int)cudaGetLastError();")
+        w("}")
 
     ELEM_BYTES = {"double": 8, "long long": 8, "int64_t": 8, "unsigned long long": 8,
                   "float": 4, "int": 4, "unsigned int": 4, "unsigned": 4, "int32_t": 4,
@@ -854,6 +921,9 @@ class Translator:
         w("  ob2_loop L;")
         w("  if (!ob2_loop_begin(&L, name, block, dim, range, args, %d)) return;" % na)
         w("  %s p;" % P)
+        # zeroed: the block is compared byte for byte (graph replay), so its
+        # padding must not carry stack contents
+        w("  memset((void *)&p, 0, sizeof(p));")
         w("  p.lo0 = L.lo[0]; p.lo1 = L.lo[1]; p.lo2 = L.lo[2];")
         w("  p.hi0 = L.hi[0]; p.hi1 = L.hi[1]; p.hi2 = L.hi[2];")
         w("  p.counter = L.counter;")
@@ -901,6 +971,10 @@ class Translator:
         else:
             w("  const ob2_mlauncher mfn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
               " : (L.idx32 ? %s_t_t : %s_t_f);" % (MN, MN, MN, MN))
+        if not reds:
+            w("  L.fuse_id = %d;" % len(self.fuse_items))
+            w("  L.ffn = ob2f_launch;")
+            self.fuse_items.append((P, "ob2b_" + loop.stub[len("ops_par_loop_"):]))
         w("  ob2_launch(&L, fn, mfn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")
         w("}")
