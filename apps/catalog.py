@@ -73,6 +73,7 @@ APPS = {
     # reference applications written with the original OPS_ACCn kernel API
     # (b200 flavour only: the oracle restates the ACC<> API)
     "ref_tealeaf": ("ref", os.path.join(REF, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
+    "ref_mgrid": ("ref", os.path.join(REF, "apps", "c", "mgrid"), ["mgrid.cpp"], None),
     "ref_cloverleaf3d": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
                          None),
     "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,

@@ -71,6 +71,10 @@ typedef struct ob2_loop {
                                offsets fit 32-bit arithmetic */
   int tune;                 /* >= 0: this launch times block-shape candidate
                                `tune` of the autotuner (OPS_B200_AUTOTUNE) */
+  unsigned prolong_mask;    /* set by the stub BEFORE ob2_loop_begin: bit i =
+                               argument i has a prolong stencil and the
+                               generated code divides the loop index by its
+                               multigrid stride */
   int fuse_id;              /* the loop's id in the fused launcher, -1: none */
   ob2_flauncher ffn;        /* the application's fused launcher (set by the
                                stub before ob2_launch; NULL: none) */

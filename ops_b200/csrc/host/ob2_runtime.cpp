@@ -121,7 +121,7 @@ struct Runtime {
   // by the stencil offset alone); any: other strides or long stencils (taken
   // to touch everything); sidx: the stencil (index into Runtime::stencils,
   // -1: none)
-  struct QAcc { int dat; int acc; int rmin, rmax; int flat; int sx[3]; int any; int sidx; };  // no padding: hashed as bytes
+  struct QAcc { int dat; int acc; int rmin, rmax; int flat; int sx[3]; int any; int sidx; int mg; };  // no padding: hashed as bytes
   struct QItem {
     int kind;               // 0 par_loop, 1 halo group
     ob2_launcher fn;
@@ -446,8 +446,10 @@ void run_tiled(std::vector<Runtime::QItem> &q, size_t b, size_t e) {
 
 bool tileable(const Runtime::QItem &it) {
   if (it.kind != 0 || it.ndim < 2) return false;
-  for (auto &a : it.acc)
+  for (auto &a : it.acc) {
     if (a.flat && a.acc != OPS_READ) return false;  // shared across tiles
+    if (a.mg) return false;  // multigrid: the dat's rows are not the loop's
+  }
   return true;
 }
 
@@ -777,6 +779,8 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
       if (st != 0 && st != 1) qa.any = 1;
     }
     if (a.stencil && a.stencil->points > 32) qa.any = 1;  // keeps the test short
+    qa.mg = (a.stencil && a.stencil->type != 0) ? 1 : 0;  // restrict / prolong
+    if (qa.mg) qa.any = 1;
     it.acc.push_back(qa);
   }
   r.q.push_back(std::move(it));
@@ -1138,13 +1142,28 @@ OPS_API ops_stencil ops_decl_strided_stencil(int dims, int points, int *sten, in
                                              char const *name) {
   return make_stencil(dims, points, sten, stride, name, 0);
 }
-OPS_API ops_stencil ops_decl_restrict_stencil(int, int, int *, int *, char const *) {
-  throw OPSException(OPS_NOT_IMPLEMENTED,
-                     "Error: multigrid restrict stencils are not supported by this backend");
+// multigrid stencils (ops_lib_core.cpp:736-831): the stride is kept as the
+// multigrid stride; type 2 restrict (the dat is read at index * stride, a
+// finer dat from a coarser loop), type 1 prolong (at index / stride, a
+// coarser dat from a finer loop); offsets are in the dat's own index space
+static ops_stencil make_mgrid_stencil(int dims, int points, int *sten, int *stride,
+                                      const char *name, int type) {
+  if (!stride) throw OPSException(OPS_INVALID_ARGUMENT, "Error: multigrid stencil without stride");
+  ops_stencil s = make_stencil(dims, points, sten, nullptr, name, type);
+  for (int i = 0; i < dims && i < OPS_MAX_DIM; i++) {
+    if (stride[i] < 1)
+      throw OPSException(OPS_INVALID_ARGUMENT, "Error: multigrid stencil stride must be >= 1");
+    s->mgrid_stride[i] = stride[i];
+  }
+  return s;
 }
-OPS_API ops_stencil ops_decl_prolong_stencil(int, int, int *, int *, char const *) {
-  throw OPSException(OPS_NOT_IMPLEMENTED,
-                     "Error: multigrid prolong stencils are not supported by this backend");
+OPS_API ops_stencil ops_decl_restrict_stencil(int dims, int points, int *sten, int *stride,
+                                              char const *name) {
+  return make_mgrid_stencil(dims, points, sten, stride, name, 2);
+}
+OPS_API ops_stencil ops_decl_prolong_stencil(int dims, int points, int *sten, int *stride,
+                                             char const *name) {
+  return make_mgrid_stencil(dims, points, sten, stride, name, 1);
 }
 
 /* ------------------------------------------------------------------------
@@ -1470,10 +1489,22 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
       if ((double)dat_points(d) * d->dim >= 2147483647.0) L->idx32 = 0;
       const int md = d->dim;
       const int *st = a.stencil ? a.stencil->stride : nullptr;
+      // a prolong stencil needs generated code that divides the loop index
+      // (the stub marks those arguments in prolong_mask)
+      const int stype = a.stencil ? a.stencil->type : 0;
+      if ((stype == 1) != (((L->prolong_mask >> i) & 1u) != 0)) {
+        OPSException ex(OPS_NOT_IMPLEMENTED);
+        ex << "Error: ops_par_loop " << name << " argument " << i
+           << (stype == 1 ? " has a prolong stencil that its generated code does not divide by"
+                          : " is marked as prolong but its stencil is not a prolong stencil")
+           << " (pass the stencil variable declared by ops_decl_prolong_stencil directly)";
+        throw ex;
+      }
       long long cum = 1, off = 0;
       long long step[3] = {0, 0, 0};
       for (int k = 0; k < block->dims && k < 3; k++) {
         int sk = st ? st[k] : 1;
+        if (stype == 2) sk *= a.stencil->mgrid_stride[k];  // restrict: index * stride
         off += cum * (long long)(-d->base[k] - d->d_m[k]);
         step[k] = cum * sk;
         cum *= d->size[k];

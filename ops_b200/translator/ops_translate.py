@@ -140,10 +140,12 @@ class LoopArg:
     dim: str = "1"  # dimension expression
     acc: str = "OPS_READ"
     opt: bool = False
+    stencil: str = ""  # the stencil expression of a dat argument
+    prolong: bool = False  # the stencil was declared by ops_decl_prolong_stencil
 
     def key(self) -> Tuple:
         return (self.kind, self.ctype, self.dim if self.kind != "dat" else
-                ("1" if self.dim.strip() == "1" else "n"), self.acc, self.opt)
+                ("1" if self.dim.strip() == "1" else "n"), self.acc, self.opt, self.prolong)
 
 
 @dataclass
@@ -198,11 +200,13 @@ def parse_arg(text: str, where: str) -> LoopArg:
     if fn == "ops_arg_dat":
         if len(inner) != 5:
             raise SystemExit("%s: ops_arg_dat needs 5 arguments: %s" % (where, text))
-        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip())
+        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip(),
+                       stencil=inner[2].strip())
     if fn == "ops_arg_dat_opt":
         if len(inner) != 6:
             raise SystemExit("%s: ops_arg_dat_opt needs 6 arguments: %s" % (where, text))
-        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip(), opt=True)
+        return LoopArg("dat", unquote(inner[3]), inner[1], inner[4].strip(), opt=True,
+                       stencil=inner[2].strip())
     if fn == "ops_arg_gbl":
         if len(inner) != 4:
             raise SystemExit("%s: ops_arg_gbl needs 4 arguments: %s" % (where, text))
@@ -397,6 +401,16 @@ class Translator:
                 if kd.params is not None and kd.name not in self.kernels:
                     self.kernels[kd.name] = kd
                 self.helpers.setdefault(kd.name, kd)
+        # multigrid prolong stencils (ops_lib_core.cpp:785-831): a dat argument
+        # whose stencil variable was declared by ops_decl_prolong_stencil reads
+        # its dat at the loop index divided by the multigrid stride, which the
+        # generated code computes (restrict stencils scale the index, which
+        # the runtime folds into the argument's steps)
+        self.prolong_names = set()
+        for s in self.sources:
+            for m in re.finditer(r"\b(\w+)\s*=\s*ops_decl_prolong_stencil\s*\(",
+                                 mask_comments_strings(open(s).read())):
+                self.prolong_names.add(m.group(1))
         for s in self.sources:
             src = open(s).read()
             m = re.search(r"#\s*define\s+OPS_(\d)D\b", src)
@@ -423,6 +437,9 @@ class Translator:
             except ValueError:
                 raise SystemExit("%s: ops_par_loop dim must be a literal: %s" % (where, args[3]))
             largs = [parse_arg(a, where) for a in args[5:]]
+            for a in largs:
+                if a.kind == "dat" and a.stencil in self.prolong_names:
+                    a.prolong = True
             loop = Loop(kname, ndim, largs)
             k = loop.key()
             if k not in self.loops:
@@ -718,6 +735,8 @@ class Translator:
             if a.kind == "dat":
                 w("  %s *b%d; long long wx%d, wy%d, wz%d; int ex%d, ey%d, ez%d, ed%d;" %
                   (p.base_type, i, i, i, i, i, i, i, i))
+                if a.prolong:  # multigrid stride: the loop index is divided by it
+                    w("  int mx%d, my%d, mz%d;" % (i, i, i))
                 if self.check:
                     w("  long long clo%d, chi%d;" % (i, i))
             elif a.kind == "gbl":
@@ -744,8 +763,13 @@ class Translator:
             for i, (a, p) in enumerate(zip(loop.args, kd.params)):
                 if a.kind == "dat":
                     ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
-                    off = ("(IDX32 ? (long long)(x * (int)p.wx%d + y * (int)p.wy%d + z * (int)p.wz%d)"
-                           " : x * p.wx%d + y * p.wy%d + z * p.wz%d)" % (i, i, i, i, i, i))
+                    if a.prolong:
+                        cx, cy, cz = ("(x / p.mx%d)" % i, "(y / p.my%d)" % i, "(z / p.mz%d)" % i)
+                    else:
+                        cx, cy, cz = "x", "y", "z"
+                    off = ("(IDX32 ? (long long)(%s * (int)p.wx%d + %s * (int)p.wy%d + %s * (int)p.wz%d)"
+                           " : %s * p.wx%d + %s * p.wy%d + %s * p.wz%d)" %
+                           (cx, i, cy, i, cz, i, cx, i, cy, i, cz, i))
                     # only optional arguments can carry a null dat
                     ptr = ("q%d ? q%d + %s : (%s *)0" % (i, i, off, p.base_type)) if a.opt \
                         else "q%d + %s" % (i, off)
@@ -772,7 +796,11 @@ class Translator:
             if self.check:
                 for i, (a, p) in enumerate(zip(loop.args, kd.params)):
                     if a.kind == "dat" and not p.is_acc:
-                        po = "(x * p.wx%d + y * p.wy%d + z * p.wz%d)" % (i, i, i)
+                        if a.prolong:
+                            po = ("((x / p.mx%d) * p.wx%d + (y / p.my%d) * p.wy%d +"
+                                  " (z / p.mz%d) * p.wz%d)" % (i, i, i, i, i, i))
+                        else:
+                            po = "(x * p.wx%d + y * p.wy%d + z * p.wz%d)" % (i, i, i)
                         call.append("p.clo%d - %s, p.chi%d - %s" % (i, po, i, po))
             w("  %s(%s);" % (loop.kernel, ", ".join(call)))
             w("}")
@@ -919,6 +947,8 @@ class Translator:
         w("  ops_arg args[%d] = {%s};" % (max(na, 1), ", ".join("arg%d" % i for i in range(na))
                                           or "ops_arg_idx()"))
         w("  ob2_loop L;")
+        w("  L.prolong_mask = %du;" % sum(1 << i for i, a in enumerate(loop.args)
+                                         if a.kind == "dat" and a.prolong))
         w("  if (!ob2_loop_begin(&L, name, block, dim, range, args, %d)) return;" % na)
         w("  %s p;" % P)
         # zeroed: the block is compared byte for byte (graph replay), so its
@@ -943,6 +973,10 @@ class Translator:
                   " p.wz%d = L.view[%d].wz;" % (i, p.base_type, i, i, i, i, i, i, i))
                 w("  p.ex%d = L.view[%d].ex; p.ey%d = L.view[%d].ey; p.ez%d = L.view[%d].ez;"
                   " p.ed%d = L.view[%d].ed;" % (i, i, i, i, i, i, i, i))
+                if a.prolong:
+                    w("  p.mx%d = arg%d.stencil->mgrid_stride[0];" % (i, i))
+                    w("  p.my%d = dim > 1 ? arg%d.stencil->mgrid_stride[1] : 1;" % (i, i))
+                    w("  p.mz%d = dim > 2 ? arg%d.stencil->mgrid_stride[2] : 1;" % (i, i))
                 if self.check:
                     w("  if (arg%d.dat && L.view[%d].base) {" % (i, i))
                     w("    p.clo%d = (long long)((char *)arg%d.dat->data_d - L.view[%d].base) /"

@@ -243,6 +243,17 @@ def test_reference_tealeaf_known_answer_on_b200(solver):
     assert "This test is considered PASSED" in out, out[-1500:]
 
 
+def test_reference_mgrid_known_answer_on_b200():
+    """The reference's multigrid test (apps/c/mgrid, original OPS_ACCn kernels)
+    built unchanged: a 6x6 field prolonged to 12x12 and 24x24 through prolong
+    stencils (index / 2, with the +-1 neighbours) and restricted back through
+    restrict stencils (index * 2), with periodic halo transfers in between;
+    its own checks compare every point with the exact expected value and
+    print PASSED."""
+    out = run_exe("ref_mgrid", "b200", cwd=tempfile.mkdtemp(prefix="mgrid_"))
+    assert "PASSED" in out and "FAILED" not in out, out[-1500:]
+
+
 def test_reference_cloverleaf3d_known_answer_on_b200():
     """CloverLeaf 3D (original OPS_ACCn kernel API) built unchanged: test
     problem 2, 96^3 cells, 87 steps, passes the reference's own check."""

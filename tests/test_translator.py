@@ -80,3 +80,36 @@ def test_translate_and_compile_opsunit():
                         os.path.join(out, "opsunit_kernels.cu"), "-o",
                         os.path.join(out, "k.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_prolong_stencil_arguments_divide_the_loop_index():
+    """A dat argument whose stencil variable comes from ops_decl_prolong_stencil
+    reads its dat at the loop index divided by the multigrid stride
+    (ops_translator/resources/templates/cpp/mpi_openmp/loop_host.cpp.j2:83-89);
+    the stub marks it for the runtime, and other arguments keep plain
+    indexing."""
+    d = tempfile.mkdtemp(prefix="ob2_prolong_")
+    src = os.path.join(d, "mg.cpp")
+    with open(os.path.join(d, "mg_kernels.h"), "w") as f:
+        f.write("void copy_k(const ACC<double> &c, ACC<double> &f) { f(0, 0) = c(0, 0); }\n")
+    with open(src, "w") as f:
+        f.write('#define OPS_2D\n#include "ops_seq_v2.h"\n#include "mg_kernels.h"\n'
+                "int main(int argc, char **argv) {\n"
+                "  ops_init(argc, argv, 1);\n"
+                '  ops_block g = ops_decl_block(2, "g");\n'
+                "  int s00[] = {0, 0}, st[] = {2, 2};\n"
+                '  ops_stencil S00 = ops_decl_stencil(2, 1, s00, "00");\n'
+                '  ops_stencil SP = ops_decl_prolong_stencil(2, 1, s00, st, "p");\n'
+                "  ops_dat c = 0, fi = 0; int r[] = {0, 8, 0, 8};\n"
+                '  ops_par_loop(copy_k, "copy_k", g, 2, r, ops_arg_dat(c, 1, SP, "double", OPS_READ),\n'
+                '               ops_arg_dat(fi, 1, S00, "double", OPS_WRITE));\n'
+                '  ops_par_loop(copy_k, "copy_k", g, 2, r, ops_arg_dat(c, 1, S00, "double", OPS_READ),\n'
+                '               ops_arg_dat(fi, 1, S00, "double", OPS_WRITE));\n'
+                "  ops_exit();\n}\n")
+    out = os.path.join(d, "gen")
+    Translator([src], [d], "mg", out).run()
+    cu = open(os.path.join(out, "mg_kernels.cu")).read()
+    # two loops: one with the prolong argument (mask bit 0), one without
+    assert cu.count("L.prolong_mask = 1u;") == 1 and cu.count("L.prolong_mask = 0u;") == 1
+    assert "(x / p.mx0)" in cu and "p.mx0 = arg0.stencil->mgrid_stride[0];" in cu
+    assert "(x / p.mx1)" not in cu
