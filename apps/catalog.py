@@ -74,6 +74,9 @@ APPS = {
     # (b200 flavour only: the oracle restates the ACC<> API)
     "ref_tealeaf": ("ref", os.path.join(REF, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
     "ref_mgrid": ("ref", os.path.join(REF, "apps", "c", "mgrid"), ["mgrid.cpp"], None),
+    # the reference's C++ object API test (OPS_CPP_API: OPS_instance methods)
+    "ref_multidim_cpp": ("ref", os.path.join(REF, "apps", "c", "multiDim"), ["multidim.cpp"],
+                         None),
     "ref_cloverleaf3d": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
                          None),
     "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,

@@ -115,6 +115,16 @@ typedef struct ops_block_core {
   int dims;
   char const *name;
   OPS_instance *instance;
+#ifdef __cplusplus
+  /* C++ object API (ops_lib_core.h:190-232 of the reference, OPS_CPP_API):
+   * block->decl_dat(...) = ops_decl_dat(block, ...) */
+  template <class T>
+  struct ops_dat_core *decl_dat(int data_size, int *block_size, int *base, int *d_m, int *d_p,
+                                T *data, char const *type, char const *name);
+  template <class T>
+  struct ops_dat_core *decl_dat(int data_size, int *block_size, int *base, int *d_m, int *d_p,
+                                int *stride, T *data, char const *type, char const *name);
+#endif
 } ops_block_core;
 typedef ops_block_core *ops_block;
 
@@ -186,6 +196,9 @@ typedef struct ops_halo_group_core {
   ops_halo *halos;
   int index;
   OPS_instance *instance;
+#ifdef __cplusplus
+  void halo_transfer();  /* = ops_halo_transfer(group) */
+#endif
 } ops_halo_group_core;
 typedef ops_halo_group_core *ops_halo_group;
 
@@ -198,6 +211,9 @@ typedef struct ops_reduction_core {
   char *type;
   char *name;
   OPS_instance *instance;
+#ifdef __cplusplus
+  template <class T> void get_result(T *ptr);  /* = ops_reduction_result(handle, ptr) */
+#endif
 } ops_reduction_core;
 typedef ops_reduction_core *ops_reduction;
 
@@ -212,10 +228,37 @@ class __attribute__((visibility("default"))) OPS_instance {
   int OPS_soa;
   int OPS_diags;
   int OPS_hybrid_gpu;
-  void *backend; /* backend runtime state */
+  void *backend;     /* backend runtime state */
+  std::ostream *os_; /* the stream ostream() returns (NULL: std::cout) */
+  OPS_instance() {}
+  /* C++ object API (ops_instance.cpp of the reference, OPS_CPP_API): the
+   * object an application creates becomes the library's instance (its
+   * OPS_soa and output stream are the ones used) and runs ops_init;
+   * deleting it runs ops_exit.  One instance per process. */
+  OPS_instance(int argc, char **argv, int diags = 1, std::ostream &os = std::cout);
+  ~OPS_instance();
   int is_root() { return 1; }
-  std::ostream &ostream() { return std::cout; }
+  std::ostream &ostream() { return os_ ? *os_ : std::cout; }
   void reset_power_counters() {}
+  /* member forms of the declaration API (definitions at the end) */
+  struct ops_block_core *decl_block(int dims, char const *name);
+  struct ops_stencil_core *decl_stencil(int dims, int points, int *sten, char const *name);
+  struct ops_stencil_core *decl_strided_stencil(int dims, int points, int *sten, int *stride,
+                                                char const *name);
+  struct ops_stencil_core *decl_restrict_stencil(int dims, int points, int *sten, int *stride,
+                                                 char const *name);
+  struct ops_stencil_core *decl_prolong_stencil(int dims, int points, int *sten, int *stride,
+                                                char const *name);
+  struct ops_halo_core *decl_halo(struct ops_dat_core *from, struct ops_dat_core *to,
+                                  int *iter_size, int *from_base, int *to_base, int *from_dir,
+                                  int *to_dir);
+  struct ops_halo_group_core *decl_halo_group(int nhalos, struct ops_halo_core **halos);
+  struct ops_reduction_core *decl_reduction_handle(int size, char const *type, char const *name);
+  template <class T> void decl_const(char const *name, int dim, char const *type, T *data);
+  template <class T> void update_const(char const *name, int dim, char const *type, T *data);
+  void partition(char const *routine);
+  void diagnostic_output();
+  void timing_output(std::ostream &stream);
 };
 
 /* ---------------------------------------------------------------------------
@@ -608,6 +651,79 @@ template <typename T> class ACC {
   }
 #endif
 };
+
+/* ---------------------------------------------------------------------------
+ * C++ object API: member forms of the C entry points (no counterpart in the
+ * C API; the reference's OPS_CPP_API methods, ops_lib_core.h:190-560).
+ * ------------------------------------------------------------------------- */
+/* Makes `inst` the library's instance and runs ops_init (the constructor of
+ * OPS_instance); ob2_release_instance runs ops_exit if `inst` is that
+ * instance (its destructor).  No counterpart in the reference's C API. */
+OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, char **argv, int diags);
+OPS_API void ob2_release_instance(OPS_instance *inst);
+
+inline OPS_instance::OPS_instance(int argc, char **argv, int diags, std::ostream &os)
+    : OPS_soa(0), OPS_diags(diags), OPS_hybrid_gpu(1), backend(NULL), os_(&os) {
+  ob2_adopt_instance(this, argc, argv, diags);
+}
+inline OPS_instance::~OPS_instance() { ob2_release_instance(this); }
+inline ops_block OPS_instance::decl_block(int dims, char const *name) {
+  return ops_decl_block(dims, name);
+}
+inline ops_stencil OPS_instance::decl_stencil(int dims, int points, int *sten,
+                                              char const *name) {
+  return ops_decl_stencil(dims, points, sten, name);
+}
+inline ops_stencil OPS_instance::decl_strided_stencil(int dims, int points, int *sten,
+                                                      int *stride, char const *name) {
+  return ops_decl_strided_stencil(dims, points, sten, stride, name);
+}
+inline ops_stencil OPS_instance::decl_restrict_stencil(int dims, int points, int *sten,
+                                                       int *stride, char const *name) {
+  return ops_decl_restrict_stencil(dims, points, sten, stride, name);
+}
+inline ops_stencil OPS_instance::decl_prolong_stencil(int dims, int points, int *sten,
+                                                      int *stride, char const *name) {
+  return ops_decl_prolong_stencil(dims, points, sten, stride, name);
+}
+inline ops_halo OPS_instance::decl_halo(ops_dat from, ops_dat to, int *iter_size,
+                                        int *from_base, int *to_base, int *from_dir,
+                                        int *to_dir) {
+  return ops_decl_halo(from, to, iter_size, from_base, to_base, from_dir, to_dir);
+}
+inline ops_halo_group OPS_instance::decl_halo_group(int nhalos, ops_halo *halos) {
+  return ops_decl_halo_group(nhalos, halos);
+}
+inline ops_reduction OPS_instance::decl_reduction_handle(int size, char const *type,
+                                                         char const *name) {
+  return ops_decl_reduction_handle(size, type, name);
+}
+template <class T>
+void OPS_instance::decl_const(char const *name, int dim, char const *type, T *data) {
+  ops_decl_const(name, dim, type, data);
+}
+template <class T>
+void OPS_instance::update_const(char const *name, int dim, char const *type, T *data) {
+  ops_update_const(name, dim, type, data);
+}
+inline void OPS_instance::partition(char const *routine) { ops_partition(routine); }
+inline void OPS_instance::diagnostic_output() { ops_diagnostic_output(); }
+inline void OPS_instance::timing_output(std::ostream &stream) { ops_timing_output(stream); }
+template <class T>
+ops_dat ops_block_core::decl_dat(int data_size, int *block_size, int *base, int *d_m,
+                                 int *d_p, T *data, char const *type, char const *name) {
+  return ops_decl_dat(this, data_size, block_size, base, d_m, d_p, data, type, name);
+}
+template <class T>
+ops_dat ops_block_core::decl_dat(int data_size, int *block_size, int *base, int *d_m,
+                                 int *d_p, int *stride, T *data, char const *type,
+                                 char const *name) {
+  return ops_decl_dat(this, data_size, block_size, base, d_m, d_p, stride, data, type, name);
+}
+inline void ops_halo_group_core::halo_transfer() { ops_halo_transfer(this); }
+template <class T> void ops_reduction_core::get_result(T *ptr) {
+  ops_reduction_result(this, ptr);
+}
 #endif /* __cplusplus */
 
 #endif /* OPS_B200_LIB_CORE_H */

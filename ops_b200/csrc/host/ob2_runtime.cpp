@@ -74,6 +74,7 @@ struct GroupX {
 
 struct Runtime {
   OPS_instance inst;
+  OPS_instance *user = nullptr;  // an application-created instance (C++ API)
   bool initialised = false;
   std::vector<ops_block> blocks;
   std::vector<ops_dat> dats;
@@ -158,6 +159,13 @@ Runtime &rt() {
     memset((void *)&R->inst, 0, sizeof(R->inst));
   }
   return *R;
+}
+
+// the instance whose settings apply: the one the application created with
+// the C++ object API, else the library's own
+OPS_instance &I() {
+  Runtime &r = rt();
+  return r.user ? *r.user : r.inst;
 }
 
 void check(int code, const char *what) {
@@ -787,20 +795,34 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
   if (r.max_chain > 0 && (int)r.q.size() >= r.max_chain) ob2_flush();
 }
 
-OPS_instance *OPS_instance::getOPSInstance() { return &rt().inst; }
+OPS_instance *OPS_instance::getOPSInstance() { return &I(); }
+
+OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, char **argv, int diags) {
+  Runtime &r = rt();
+  if (r.user && r.user != inst)
+    throw OPSException(OPS_INVALID_ARGUMENT, "Error: only one OPS_instance per process");
+  r.user = inst;
+  ops_init(argc, argv, diags);
+}
+
+OPS_API void ob2_release_instance(OPS_instance *inst) {
+  if (!R || rt().user != inst) return;
+  ops_exit();
+  rt().user = nullptr;
+}
 
 /* ------------------------------------------------------------------------
  * init / exit  (ops_lib_core.cpp:100-275; ops_cuda_common.cu:68-182)
  * ---------------------------------------------------------------------- */
 OPS_API void ops_init(const int argc, const char *const argv[], const int diags) {
   Runtime &r = rt();
-  r.inst.OPS_diags = diags;
-  r.inst.OPS_hybrid_gpu = 1;
+  I().OPS_diags = diags;
+  I().OPS_hybrid_gpu = 1;
   for (int i = 0; i < argc; i++) {
     if (!argv || !argv[i]) continue;
     const char *a = argv[i];
     const char *p;
-    if ((p = strstr(a, "-OPS_DIAGS="))) r.inst.OPS_diags = atoi(p + 11);
+    if ((p = strstr(a, "-OPS_DIAGS="))) I().OPS_diags = atoi(p + 11);
     if ((p = strstr(a, "OPS_BLOCK_SIZE_X="))) r.block_x = atoi(p + 17);
     if ((p = strstr(a, "OPS_BLOCK_SIZE_Y="))) r.block_y = atoi(p + 17);
     if ((p = strstr(a, "OPS_BLOCK_SIZE_Z="))) r.block_z = atoi(p + 17);
@@ -844,7 +866,7 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if (r.block_y < 1) r.block_y = 1;
   if (r.block_z < 1) r.block_z = 1;
   // diagnostics above 1: per-kernel device times in the timing table
-  if (r.inst.OPS_diags > 1) r.ktime = true;
+  if (I().OPS_diags > 1) r.ktime = true;
   if (r.initialised) return;
   check(ob2_dev_init(r.device), "ops_init (no usable CUDA device)");
   check(ob2_dev_sm_count(&r.sms), "ops_init");
@@ -875,7 +897,7 @@ OPS_API void ops_exit(void) {
   ob2_dev_sync();
 }
 
-OPS_API void ops_set_soa(const int soa) { rt().inst.OPS_soa = soa; }
+OPS_API void ops_set_soa(const int soa) { I().OPS_soa = soa; }
 
 OPS_API ops_block ops_decl_block(int dims, const char *name) {
   if (dims < 1 || dims > 3)
@@ -884,7 +906,7 @@ OPS_API ops_block ops_decl_block(int dims, const char *name) {
   ops_block b = (ops_block)calloc(1, sizeof(ops_block_core));
   b->dims = dims;
   b->name = copy_str(name);
-  b->instance = &rt().inst;
+  b->instance = &I();
   b->index = (int)rt().blocks.size();
   rt().blocks.push_back(b);
   return b;
@@ -951,7 +973,7 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
   d->dirty_hd = data ? 0 : 2;
   long long off = 0, cum = 1;
   for (int i = 0; i < block->dims; i++) {
-    off += (long long)(rt().inst.OPS_soa ? d->type_size : d->elem_size) * cum *
+    off += (long long)(I().OPS_soa ? d->type_size : d->elem_size) * cum *
            (-d->base[i] - d->d_m[i]);
     cum *= d->size[i];
   }
@@ -1090,7 +1112,7 @@ OPS_API ops_reduction ops_decl_reduction_handle(int size, const char *type, cons
   r->data = (char *)calloc(size, 1);
   r->type = copy_str(type);
   r->name = copy_str(name);
-  r->instance = &rt().inst;
+  r->instance = &I();
   r->index = (int)rt().reds.size();
   rt().reds.push_back(r);
   RedX x;
@@ -1192,7 +1214,7 @@ OPS_API ops_halo_group ops_decl_halo_group(int nhalos, ops_halo *halos) {
   g->nhalos = nhalos;
   g->halos = (ops_halo *)malloc(sizeof(ops_halo) * (nhalos > 0 ? nhalos : 1));
   for (int i = 0; i < nhalos; i++) g->halos[i] = halos[i];
-  g->instance = &rt().inst;
+  g->instance = &I();
   g->index = (int)rt().groups.size();
   rt().groups.push_back(g);
   rt().groupx.push_back(GroupX());
@@ -1225,7 +1247,7 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
       t.float_kind = 1;
     }
     t.ncomp = h->from->dim;
-    t.src_soa = t.dst_soa = rt().inst.OPS_soa;
+    t.src_soa = t.dst_soa = I().OPS_soa;
     t.npts = 1;
     for (int a = 0; a < 3; a++) {
       t.iter[a] = h->iter_size[a];
@@ -1449,7 +1471,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   size_t red_bytes = 0;
   int nred = 0;
   L->idx32 = 1;
-  const int soa = r.inst.OPS_soa;
+  const int soa = I().OPS_soa;
   for (int i = 0; i < nargs; i++) {
     ops_arg &a = args[i];
     ob2_view &v = L->view[i];
@@ -1698,7 +1720,7 @@ OPS_API void ops_fprintf(FILE *f, const char *fmt, ...) {
 }
 OPS_API void ops_diagnostic_output(void) {
   Runtime &r = rt();
-  if (r.inst.OPS_diags <= 1) return;
+  if (I().OPS_diags <= 1) return;
   printf("\n OPS diagnostic output (B200 backend)\n --------------------------------\n");
   printf(" blocks %zu, dats %zu, stencils %zu, halos %zu\n", r.blocks.size(), r.dats.size(),
          r.stencils.size(), r.halos.size());
@@ -1782,7 +1804,7 @@ OPS_API void ops_NaNcheck(ops_dat d) {
   ob2_flush();
   put_data(d);
   long long first = -1;
-  check(ob2_nan_find(d->data_d, d->type_size, d->dim, rt().inst.OPS_soa, d->mem / d->type_size,
+  check(ob2_nan_find(d->data_d, d->type_size, d->dim, I().OPS_soa, d->mem / d->type_size,
                      &first),
         "ops_NaNcheck");
   if (first < 0) return;
@@ -1975,7 +1997,7 @@ static void slab_io(ops_dat d, char *data, const int *range, ops_memspace ms, in
     buf = rt().stage_d;
     if (dir == 1) check(ob2_dev_h2d(buf, data, bytes), "ops_dat_set_data");
   }
-  check(ob2_box_copy(d->data_d, d->type_size, d->dim, rt().inst.OPS_soa, size3, start, count,
+  check(ob2_box_copy(d->data_d, d->type_size, d->dim, I().OPS_soa, size3, start, count,
                      buf, dir),
         dir == 0 ? "ops_dat_fetch_data" : "ops_dat_set_data");
   if (ms != OPS_DEVICE && dir == 0) check(ob2_dev_d2h(data, buf, bytes), "ops_dat_fetch_data");
@@ -2130,7 +2152,7 @@ OPS_API void ops_dump_dats(const char *path) {
     int tl = (int)strlen(d->type);
     fwrite(&tl, 4, 1, f);
     fwrite(d->type, 1, tl, f);
-    int meta[4] = {d->dim, d->type_size, d->block->dims, rt().inst.OPS_soa};
+    int meta[4] = {d->dim, d->type_size, d->block->dims, I().OPS_soa};
     fwrite(meta, 4, 4, f);
     fwrite(d->size, 4, OPS_MAX_DIM, f);
     fwrite(d->d_m, 4, OPS_MAX_DIM, f);

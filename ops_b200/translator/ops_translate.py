@@ -447,8 +447,16 @@ class Translator:
             self.loops[k].sources.append(where)
             sites.append((start, end, k, args))
         self.call_sites[path] = sites
-        for fn in ("ops_decl_const", "ops_decl_const2", "ops_update_const"):
-            for _, _, args in find_calls(src, fn):
+        # free calls, and the member calls of the C++ object API
+        # (instance->decl_const(...), instance->update_const(...))
+        member = []
+        masked = mask_comments_strings(src)
+        for m in re.finditer(r"(?:->|\.)\s*(?:decl_const|update_const)\s*\(", masked):
+            op = m.end() - 1
+            cl = match_paren(masked, op)
+            member.append((m.start(), cl + 1, split_top(src[op + 1:cl], masked[op + 1:cl])))
+        for fn in ("ops_decl_const", "ops_decl_const2", "ops_update_const", None):
+            for _, _, args in (find_calls(src, fn) if fn else member):
                 if len(args) != 4:
                     continue
                 name = unquote(args[0])
@@ -631,6 +639,17 @@ class Translator:
         with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
             f.write("\n".join(L) + "\n")
 
+    GBL_CAP = 64  # elements kept for a global array whose length is a run-time value
+
+    def gbl_extent(self, dim: str) -> str:
+        """The parameter-block extent of an OPS_READ global: its length when
+        that is a compile-time expression (literals and macro names), else
+        GBL_CAP elements (the stub rejects longer arrays at run time)."""
+        d = dim.strip()
+        if re.fullmatch(r"[0-9A-Z_\s\*\+\-\(\)]+", d):
+            return d
+        return str(self.GBL_CAP)
+
     def emit_fused(self, w) -> None:
         """One kernel that runs several different loops of the application
         in one launch (the runtime passes only loops whose footprints do not
@@ -740,7 +759,7 @@ class Translator:
                 if self.check:
                     w("  long long clo%d, chi%d;" % (i, i))
             elif a.kind == "gbl":
-                w("  %s g%d[%s];" % (p.base_type, i, a.dim))
+                w("  %s g%d[%s];" % (p.base_type, i, self.gbl_extent(a.dim)))
             elif a.kind == "reduce":
                 w("  %s *r%d; %s *part%d; int first%d;" % (p.base_type, i, p.base_type, i, i))
                 reds.append((i, a, p))

@@ -254,6 +254,18 @@ def test_reference_mgrid_known_answer_on_b200():
     assert "PASSED" in out and "FAILED" not in out, out[-1500:]
 
 
+def test_reference_cpp_object_api_multidim_on_b200():
+    """The reference's C++ object API test (apps/c/multiDim: OPS_instance
+    created by the application with its own output stream, SoA storage set on
+    the instance, instance->decl_* calls, block->decl_dat, halo_group->
+    halo_transfer, reduction->get_result, globals whose length is a run-time
+    value) built unchanged: its two-component reduction matches the expected
+    value and it prints PASSED."""
+    out = run_exe("ref_multidim_cpp", "b200", cwd=tempfile.mkdtemp(prefix="multidim_"))
+    assert "This test is considered PASSED" in out, out[-1500:]
+    assert "The test using ops_arg_gbl arguments passed!" in out
+
+
 def test_reference_cloverleaf3d_known_answer_on_b200():
     """CloverLeaf 3D (original OPS_ACCn kernel API) built unchanged: test
     problem 2, 96^3 cells, 87 steps, passes the reference's own check."""

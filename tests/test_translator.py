@@ -113,3 +113,34 @@ def test_prolong_stencil_arguments_divide_the_loop_index():
     assert cu.count("L.prolong_mask = 1u;") == 1 and cu.count("L.prolong_mask = 0u;") == 1
     assert "(x / p.mx0)" in cu and "p.mx0 = arg0.stencil->mgrid_stride[0];" in cu
     assert "(x / p.mx1)" not in cu
+
+
+def test_cpp_api_constants_and_runtime_length_globals():
+    """Constants declared through the C++ object API (instance->decl_const)
+    become device constants like ops_decl_const ones; an ops_arg_gbl whose
+    length is a run-time variable gets a fixed-capacity slot in the parameter
+    block (the stub rejects longer arrays), one with a literal or macro
+    length keeps that length."""
+    d = tempfile.mkdtemp(prefix="ob2_cppapi_")
+    src = os.path.join(d, "c.cpp")
+    with open(os.path.join(d, "c_kernels.h"), "w") as f:
+        f.write("void k(ACC<double> &u, const double *a, const double *b) {"
+                " u(0, 0) = a[0] + b[0] + kc; }\n")
+    with open(src, "w") as f:
+        f.write('#define OPS_2D\n#define OPS_CPP_API\n#include "ops_seq_v2.h"\n'
+                "int kc = 3;\n#define NB 4\n"
+                '#include "c_kernels.h"\n'
+                "int main(int argc, char **argv) {\n"
+                "  OPS_instance *instance = new OPS_instance(argc, argv, 1);\n"
+                '  instance->decl_const("kc", 1, "int", &kc);\n'
+                "  ops_block g = 0; ops_dat u = 0; ops_stencil S = 0; int n = 5;\n"
+                "  double a[5], b[NB]; int r[] = {0, 4, 0, 4};\n"
+                '  ops_par_loop(k, "k", g, 2, r, ops_arg_dat(u, 1, S, "double", OPS_WRITE),\n'
+                '               ops_arg_gbl(a, n, "double", OPS_READ),\n'
+                '               ops_arg_gbl(b, NB, "double", OPS_READ));\n'
+                "  delete instance;\n}\n")
+    out = os.path.join(d, "gen")
+    Translator([src], [d], "c", out).run()
+    cu = open(os.path.join(out, "c_kernels.cu")).read()
+    assert "__constant__ int kc;" in cu
+    assert "double g1[64];" in cu and "double g2[NB];" in cu
