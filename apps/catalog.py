@@ -77,6 +77,7 @@ APPS = {
     # the reference's C++ object API test (OPS_CPP_API: OPS_instance methods)
     "ref_multidim_cpp": ("ref", os.path.join(REF, "apps", "c", "multiDim"), ["multidim.cpp"],
                          None),
+    "ref_mb_trid": ("ref", os.path.join(REF, "apps", "c", "mb_trid_test"), ["mb_trid.cpp"], None),
     "ref_cloverleaf3d": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
                          None),
     "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,

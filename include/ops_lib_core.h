@@ -235,7 +235,8 @@ class __attribute__((visibility("default"))) OPS_instance {
    * object an application creates becomes the library's instance (its
    * OPS_soa and output stream are the ones used) and runs ops_init;
    * deleting it runs ops_exit.  One instance per process. */
-  OPS_instance(int argc, char **argv, int diags = 1, std::ostream &os = std::cout);
+  OPS_instance(const int argc, const char *const argv[], const int diags = 1,
+               std::ostream &os = std::cout);
   ~OPS_instance();
   int is_root() { return 1; }
   std::ostream &ostream() { return os_ ? *os_ : std::cout; }
@@ -659,10 +660,12 @@ template <typename T> class ACC {
 /* Makes `inst` the library's instance and runs ops_init (the constructor of
  * OPS_instance); ob2_release_instance runs ops_exit if `inst` is that
  * instance (its destructor).  No counterpart in the reference's C API. */
-OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, char **argv, int diags);
+OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, const char *const *argv,
+                                int diags);
 OPS_API void ob2_release_instance(OPS_instance *inst);
 
-inline OPS_instance::OPS_instance(int argc, char **argv, int diags, std::ostream &os)
+inline OPS_instance::OPS_instance(const int argc, const char *const argv[], const int diags,
+                                  std::ostream &os)
     : OPS_soa(0), OPS_diags(diags), OPS_hybrid_gpu(1), backend(NULL), os_(&os) {
   ob2_adopt_instance(this, argc, argv, diags);
 }

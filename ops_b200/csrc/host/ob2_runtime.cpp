@@ -797,7 +797,8 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
 
 OPS_instance *OPS_instance::getOPSInstance() { return &I(); }
 
-OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, char **argv, int diags) {
+OPS_API void ob2_adopt_instance(OPS_instance *inst, int argc, const char *const *argv,
+                                int diags) {
   Runtime &r = rt();
   if (r.user && r.user != inst)
     throw OPSException(OPS_INVALID_ARGUMENT, "Error: only one OPS_instance per process");

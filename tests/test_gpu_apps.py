@@ -266,6 +266,13 @@ def test_reference_cpp_object_api_multidim_on_b200():
     assert "The test using ops_arg_gbl arguments passed!" in out
 
 
+def test_reference_mb_trid_regression_on_b200():
+    """The reference's mb_trid_test (C++ object API with `const char **argv`,
+    two blocks, an ops_tridsolver_params per block, everything deleted again):
+    a regression case for a crash in the reference; it must run to the end."""
+    run_exe("ref_mb_trid", "b200", cwd=tempfile.mkdtemp(prefix="mbtrid_"))
+
+
 def test_reference_cloverleaf3d_known_answer_on_b200():
     """CloverLeaf 3D (original OPS_ACCn kernel API) built unchanged: test
     problem 2, 96^3 cells, 87 steps, passes the reference's own check."""
