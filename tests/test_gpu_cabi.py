@@ -202,3 +202,51 @@ def test_trid_strided_kernels(mode, typ):
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                        env=dict(os.environ, OB2_TRID_STRIDED=mode), timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+def test_device_memspace_slab_set_and_fetch():
+    """The external data access API with device buffers (OPS_DEVICE), as the
+    reference's access app uses it (apps/c/access/fetch_data.cu): a 2 x 2 slab
+    set from device memory, the whole interior and another slab fetched into
+    device memory, checked against numpy."""
+    from tests import cabi
+    L = cabi.lib()
+    vp, ip = C.c_void_p, C.POINTER(C.c_int)
+    L.ops_dat_set_data_slab_memspace.argtypes = [vp, C.c_int, vp, ip, C.c_int]
+    L.ops_dat_fetch_data_slab_memspace.argtypes = [vp, C.c_int, vp, ip, C.c_int]
+    L.ops_dat_fetch_data_memspace.argtypes = [vp, C.c_int, vp, C.c_int]
+    L.ob2_dev_malloc.argtypes = [C.POINTER(vp), C.c_size_t]
+    L.ob2_dev_free.argtypes = [vp]
+    L.ob2_dev_h2d.argtypes = [vp, vp, C.c_size_t]
+    L.ob2_dev_d2h.argtypes = [vp, vp, C.c_size_t]
+    OPS_DEVICE = 2
+    blk = L.ops_decl_block(2, b"access")
+    dat = cabi.Dat(blk, 2, [20, 20], [-1, -1], [1, 1], "double", "data0")
+    interior = np.add.outer(100.0 * np.arange(20), np.arange(20.0))  # [y, x] = x + 100 y
+    dat.set_interior(interior)
+    want = interior.copy()
+
+    def dev(nbytes):
+        p = vp()
+        assert L.ob2_dev_malloc(C.byref(p), nbytes) == 0
+        return p
+
+    slab_in = np.array([-1.0, -2.0, -3.0, -4.0])
+    d_in = dev(32)
+    assert L.ob2_dev_h2d(d_in, slab_in.ctypes.data, 32) == 0
+    L.ops_dat_set_data_slab_memspace(dat.h, 0, d_in, cabi.ivec([6, 8, 6, 8]), OPS_DEVICE)
+    want[6:8, 6:8] = slab_in.reshape(2, 2)
+
+    d_all = dev(20 * 20 * 8)
+    L.ops_dat_fetch_data_memspace(dat.h, 0, d_all, OPS_DEVICE)
+    got = np.empty((20, 20))
+    assert L.ob2_dev_d2h(got.ctypes.data, d_all, got.nbytes) == 0
+    assert np.array_equal(got, want)
+
+    d_slab = dev(32)
+    L.ops_dat_fetch_data_slab_memspace(dat.h, 0, d_slab, cabi.ivec([10, 12, 10, 12]), OPS_DEVICE)
+    slab_out = np.empty(4)
+    assert L.ob2_dev_d2h(slab_out.ctypes.data, d_slab, 32) == 0
+    assert np.array_equal(slab_out, want[10:12, 10:12].ravel())
+    for p in (d_in, d_all, d_slab):
+        L.ob2_dev_free(p)
