@@ -9,9 +9,11 @@ Flavours
 
 Applications are either this repository's drivers under apps/ (our code, on the
 unchanged OPS API) or reference applications, whose sources are read from the
-reference tree at build time only.  Every build of a reference application,
-and every ref_* flavour, goes under oracle/_ref/ (git-ignored; the built
-binaries travel to the GPU machine, the sources do not).
+reference tree named by OPS_REFERENCE_TREE at build time only (without it,
+only the prebuilt binaries are used).  Product builds (the b200 flavour) of
+reference applications go under apps/_build/ref/; the checker builds (the
+oracle flavour and every ref_* flavour) go under oracle/_ref/.  Both are
+git-ignored; the built binaries travel to the GPU machine, the sources do not.
 """
 
 from __future__ import annotations
@@ -24,7 +26,10 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
-REF = os.environ.get("OPS_REFERENCE_TREE", "/root/reference")
+# the upstream OPS tree, read at build time only; unset: nothing is rebuilt
+# from it, and the reference-derived builds already present are used as they are
+REF = os.environ.get("OPS_REFERENCE_TREE", "")
+_REF_ROOT = REF or os.path.join(os.sep, "nonexistent-ops-reference-tree")
 ORACLE_LIB_DIR = os.path.join(ROOT, "oracle", "_build")
 REF_OUT = os.path.join(ROOT, "oracle", "_ref")
 
@@ -51,48 +56,52 @@ APPS = {
     "adi3d": ("own", os.path.join(ROOT, "apps", "adi3d"), ["adi3d.cpp"], None),
     "heat_cg": ("own", os.path.join(ROOT, "apps", "heat_cg"), ["heat_cg.cpp"], None),
     "opsunit": ("own", os.path.join(ROOT, "apps", "opsunit"), ["opsunit.cpp"], None),
-    "ref_poisson": ("ref", os.path.join(REF, "apps", "c", "poisson"), ["poisson.cpp"], None),
-    "ref_mblock": ("ref", os.path.join(REF, "apps", "c", "mblock"), ["mblock.cpp"], None),
-    "ref_laplace": ("ref", os.path.join(REF, "apps", "c", "laplace2d_tutorial", "step7"),
+    "ref_poisson": ("ref", os.path.join(_REF_ROOT, "apps", "c", "poisson"), ["poisson.cpp"], None),
+    "ref_mblock": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mblock"), ["mblock.cpp"], None),
+    "ref_laplace": ("ref", os.path.join(_REF_ROOT, "apps", "c", "laplace2d_tutorial", "step7"),
                     ["laplace2d.cpp"], None),
     # further reference applications, built unchanged (the v2 ACC API)
-    "ref_lowdim": ("ref", os.path.join(REF, "apps", "c", "lowdim_test"), ["lowdim.cpp"], None),
-    "ref_multidim3d": ("ref", os.path.join(REF, "apps", "c", "multiDim3D"), ["multidim.cpp"],
+    "ref_lowdim": ("ref", os.path.join(_REF_ROOT, "apps", "c", "lowdim_test"), ["lowdim.cpp"], None),
+    "ref_multidim3d": ("ref", os.path.join(_REF_ROOT, "apps", "c", "multiDim3D"), ["multidim.cpp"],
                        None),
-    "ref_shsgc": ("ref", os.path.join(REF, "apps", "c", "shsgc"), ["shsgc.cpp"], None),
-    "ref_compact": ("ref", os.path.join(REF, "apps", "c", "compact_scheme"),
+    "ref_shsgc": ("ref", os.path.join(_REF_ROOT, "apps", "c", "shsgc"), ["shsgc.cpp"], None),
+    "ref_compact": ("ref", os.path.join(_REF_ROOT, "apps", "c", "compact_scheme"),
                     ["compact_scheme.cpp"], None),
-    "ref_random": ("ref", os.path.join(REF, "apps", "c", "random"), ["random.cpp"], None),
-    "ref_tiling_fix": ("ref", os.path.join(REF, "apps", "c", "tiling_fix"), ["minisenga.cpp"],
+    "ref_random": ("ref", os.path.join(_REF_ROOT, "apps", "c", "random"), ["random.cpp"], None),
+    "ref_tiling_fix": ("ref", os.path.join(_REF_ROOT, "apps", "c", "tiling_fix"), ["minisenga.cpp"],
                        None),
-    "ref_adi_burger": ("ref", os.path.join(REF, "apps", "c", "adi_burger"), ["adi_burger.cpp"],
+    "ref_adi_burger": ("ref", os.path.join(_REF_ROOT, "apps", "c", "adi_burger"), ["adi_burger.cpp"],
                        None),
-    "ref_adi_burger3d": ("ref", os.path.join(REF, "apps", "c", "adi_burger_3D"),
+    "ref_adi_burger3d": ("ref", os.path.join(_REF_ROOT, "apps", "c", "adi_burger_3D"),
                          ["adi_burger_3D.cpp"], None),
-    "ref_tti": ("ref", os.path.join(REF, "apps", "c", "tti"), ["tti.cpp"], None),
+    "ref_tti": ("ref", os.path.join(_REF_ROOT, "apps", "c", "tti"), ["tti.cpp"], None),
     # reference applications written with the original OPS_ACCn kernel API
     # (b200 flavour only: the oracle restates the ACC<> API)
-    "ref_tealeaf": ("ref", os.path.join(REF, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
-    "ref_mgrid": ("ref", os.path.join(REF, "apps", "c", "mgrid"), ["mgrid.cpp"], None),
+    "ref_tealeaf": ("ref", os.path.join(_REF_ROOT, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
+    "ref_mgrid": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mgrid"), ["mgrid.cpp"], None),
     # the reference's C++ object API test (OPS_CPP_API: OPS_instance methods)
-    "ref_multidim_cpp": ("ref", os.path.join(REF, "apps", "c", "multiDim"), ["multidim.cpp"],
+    "ref_multidim_cpp": ("ref", os.path.join(_REF_ROOT, "apps", "c", "multiDim"), ["multidim.cpp"],
                          None),
-    "ref_mb_trid": ("ref", os.path.join(REF, "apps", "c", "mb_trid_test"), ["mb_trid.cpp"], None),
-    "ref_cloverleaf3d": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
+    "ref_mb_trid": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mb_trid_test"), ["mb_trid.cpp"], None),
+    "ref_cloverleaf3d": ("ref", os.path.join(_REF_ROOT, "apps", "c", "CloverLeaf_3D"), CLOVER3D_SRCS,
                          None),
-    "cloverleaf": ("ref", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
+    "cloverleaf": ("ref", os.path.join(_REF_ROOT, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
                    CLOVER_SRCS[:15]),
     # the CloverLeaf step harness: the CloverLeaf sources plus apps/clover_step
-    "clover_step": ("mixed", os.path.join(REF, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
+    "clover_step": ("mixed", os.path.join(_REF_ROOT, "apps", "c", "CloverLeaf"), CLOVER_SRCS,
                     CLOVER_SRCS[:15]),
 }
 CLOVER_STEP_SRC = os.path.join(ROOT, "apps", "clover_step", "clover_step.cpp")
+# shared headers of this repository's drivers and harnesses (apps/dumpdats.h)
+APPS_DIR = os.path.join(ROOT, "apps")
 
 
 def build_dir(name: str, flavour: str) -> str:
     kind = APPS[name][0]
     if kind == "own" and not flavour.startswith("ref_"):
         return os.path.join(ROOT, "apps", name, "_build", flavour)
+    if flavour == "b200":  # product build of a reference application
+        return os.path.join(ROOT, "apps", "_build", "ref", name, flavour)
     return os.path.join(REF_OUT, "apps", name, flavour)
 
 
@@ -128,8 +137,11 @@ def ensure_oracle_lib() -> str:
 
 
 def ensure_ref_lib() -> str:
-    if not os.path.isdir(REF):
-        raise RuntimeError("reference tree not present")
+    if not REF or not os.path.isdir(REF):
+        lib = os.path.join(REF_OUT, "lib", "libops_seq.a")
+        if os.path.exists(lib):
+            return lib
+        raise RuntimeError("reference tree not present (set OPS_REFERENCE_TREE)")
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "lib", "-j8", "REF=" + REF])
     return os.path.join(REF_OUT, "lib", "libops_seq.a")
 
@@ -157,6 +169,8 @@ def stale(name: str, flavour: str, shared: bool = False) -> bool:
         return True
     if not available(name):
         return False  # prebuilt and no sources to rebuild from
+    if flavour.startswith("ref_") and not REF:
+        return False  # prebuilt against the reference tree, which is not named
     t = os.path.getmtime(target)
     return any(os.path.getmtime(p) > t for p in _deps(name, flavour))
 
@@ -179,11 +193,11 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
         if name == "clover_step":
             # only clover_leaf.cpp's main is renamed; the harness keeps its own
             return _build_b200_clover_step(out, d, paths, shared)
-        return b200_build(name, out, paths, [d], defines=defs, shared=shared)
+        return b200_build(name, out, paths, [d, APPS_DIR], defines=defs, shared=shared)
     if flavour == "oracle":
         lib = ensure_oracle_lib()
         inc = ["-I" + os.path.join(ROOT, "oracle", "include"), "-I" + os.path.join(ROOT, "include"),
-               "-I" + d]
+               "-I" + d, "-I" + APPS_DIR]
         objs = []
         for p in paths:
             o = os.path.join(out, os.path.basename(p) + ".o")
@@ -212,7 +226,8 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
                 shutil.copy(os.path.join(d, f), srcdir)
         objs_src = [os.path.join(srcdir, os.path.basename(p)) for p in paths
                     if p != CLOVER_STEP_SRC]
-        flags = ["-O3", "-std=c++14", "-fPIC", "-w", "-fopenmp", "-Dgnu", "-I" + rinc, "-I" + srcdir]
+        flags = ["-O3", "-std=c++14", "-fPIC", "-w", "-fopenmp", "-Dgnu", "-I" + rinc, "-I" + srcdir,
+                 "-I" + APPS_DIR]
         if flavour == "ref_omp":
             trans = APPS[name][3] or APPS[name][2]
             _run([sys.executable, os.path.join(REF, "ops_translator_legacy", "c", "ops.py"),
@@ -242,7 +257,7 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
 
 def _build_b200_clover_step(out, d, paths, shared):
     from ops_b200.build_app import build as b200_build
-    return b200_build("clover_step", out, paths, [d], defines=[], shared=shared,
+    return b200_build("clover_step", out, paths, [d, APPS_DIR], defines=[], shared=shared,
                       rename_main={"clover_leaf.cpp": "clover_leaf_main"})
 
 

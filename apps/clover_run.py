@@ -1,14 +1,21 @@
 """Run the CloverLeaf step harness (apps/clover_step) in one flavour.
 
     python -m apps.clover_run --flavour b200|oracle|ref_omp --cells N --steps K
-                              [--warmup W] [--seed S] [--dump FILE] [--threads T]
+                              [--warmup W] [--seed S] [--dump FILE] [--fetch-dump FILE]
+                              [--threads T]
 
 Writes the input deck of the 2D hydro configuration into a scratch directory
 (background rho=0.2 e=1.0 on a 10x10 domain, a cell-aligned 2.5x2.5 square of
 rho=1.0 e=2.5 whose position is drawn from the seed), runs W untimed and K
 timed steps through the harness's C entry points, and prints one JSON line:
 the field summary of the final state (volume, mass, pressure, internal and
-kinetic energy), the per-step time and the steps run.
+kinetic energy), the per-step time and the steps run.  The field summary is
+taken after the timed steps, outside the timed region.
+
+--dump writes every live dat with halos at ops_exit (this backend and the
+oracle only); --fetch-dump writes every dat's interior through
+ops_dat_fetch_data (clover_step_dump), which works on every flavour, the
+reference's OpenMP backend included.
 
 Each flavour runs in its own process (every flavour exports the same OPS
 symbols).
@@ -71,6 +78,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=0)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--dump", default=None)
+    ap.add_argument("--fetch-dump", default=None)
     ap.add_argument("--threads", type=int, default=0)
     a = ap.parse_args(argv)
     from apps.catalog import artifact
@@ -81,6 +89,8 @@ def main(argv=None):
         os.environ["OMP_NUM_THREADS"] = str(a.threads)
     if a.dump:
         os.environ["OPS_DUMP_FILE"] = os.path.abspath(a.dump)
+    if a.fetch_dump:
+        a.fetch_dump = os.path.abspath(a.fetch_dump)
     work = tempfile.mkdtemp(prefix="clover_")
     with open(os.path.join(work, "clover.in"), "w") as f:
         f.write(make_deck(a.cells, a.seed))
@@ -93,8 +103,12 @@ def main(argv=None):
         L.clover_step_run(a.warmup)
     t0 = time.perf_counter()
     L.clover_step_run(a.steps)
-    L.clover_step_summary()
     t1 = time.perf_counter()
+    L.clover_step_summary()
+    if a.fetch_dump:
+        L.clover_step_dump.argtypes = [ctypes.c_char_p]
+        if L.clover_step_dump(a.fetch_dump.encode()) != 0:
+            raise SystemExit("clover_step_dump failed")
     L.clover_step_finish()
     summ = parse_summary(open(os.path.join(work, "clover.out")).read())
     print(json.dumps({"flavour": a.flavour, "cells": a.cells, "steps": a.steps,

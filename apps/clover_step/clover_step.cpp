@@ -22,6 +22,7 @@
 #include "ops_seq_v2.h"
 #include "data.h"
 #include "definitions.h"
+#include "dumpdats.h"
 
 void initialise();
 void field_summary();
@@ -88,6 +89,44 @@ __attribute__((visibility("default"))) void clover_step_summary(void) {
 }
 
 __attribute__((visibility("default"))) int clover_step_current(void) { return step; }
+
+/* Every dat of the application (build_field.cpp) written to `path` through
+ * ops_dat_fetch_data (apps/dumpdats.h): interiors, the same on every backend. */
+__attribute__((visibility("default"))) int clover_step_dump(const char *path) {
+  ops_dat all[] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
+                   volume, xvel0, xvel1, yvel0, yvel1, vol_flux_x, vol_flux_y, mass_flux_x,
+                   mass_flux_y, xarea, yarea, work_array1, work_array2, work_array3,
+                   work_array4, work_array5, work_array6, work_array7, cellx, celly, vertexx,
+                   vertexy, celldx, celldy, vertexdx, vertexdy, xx, yy};
+  return dump_dats(path, all, (int)(sizeof(all) / sizeof(all[0])));
+}
+
+/* Moves every dat of the application between the device and host buffers
+ * through the public data-access calls: dir 0 fetches each dat's interior
+ * into bufs[i], dir 1 sets it from bufs[i].  Returns the dat count (with
+ * bufs == NULL: the count, and the byte size of each into sizes). */
+__attribute__((visibility("default"))) int clover_step_state(int dir, char **bufs,
+                                                             long long *sizes) {
+  ops_dat all[] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
+                   volume, xvel0, xvel1, yvel0, yvel1, vol_flux_x, vol_flux_y, mass_flux_x,
+                   mass_flux_y, xarea, yarea, work_array1, work_array2, work_array3,
+                   work_array4, work_array5, work_array6, work_array7, cellx, celly, vertexx,
+                   vertexy, celldx, celldy, vertexdx, vertexdy, xx, yy};
+  const int n = (int)(sizeof(all) / sizeof(all[0]));
+  for (int i = 0; i < n; i++) {
+    if (!bufs) {
+      int disp[2], ext[2];
+      ops_dat_get_extents(all[i], 0, disp, ext);
+      if (sizes) sizes[i] = (long long)ext[0] * ext[1] * all[i]->elem_size;
+      continue;
+    }
+    if (dir == 0)
+      ops_dat_fetch_data(all[i], 0, bufs[i]);
+    else
+      ops_dat_set_data(all[i], 0, bufs[i]);
+  }
+  return n;
+}
 
 __attribute__((visibility("default"))) void clover_step_finish(void) {
   fflush(g_out);

@@ -19,6 +19,7 @@
  *          -tol= (default 1e-10) -inner= (residual drop between FP64
  *          residual replacements, default 1e-2)
  *          -maxit= (iteration cap per CG, default 20000) -dt= (default 4e-6)
+ *          -dump=FILE (every dat's interior at the end, apps/dumpdats.h)
  *          -seed= (circle centre, default 4) -useed= (u0, default 5)
  * Prints per solver: iterations, recursive and true relative residuals and a
  * checksum ("fp64 ...", "mixed ..."), for both the relative difference of the
@@ -39,6 +40,7 @@ float hc_rx32, hc_ry32;
 int hc_seed;
 
 #include "heat_cg_kernels.h"
+#include "dumpdats.h"
 
 static const char *sopt(int argc, char **argv, const char *key) {
   size_t n = strlen(key);
@@ -284,6 +286,7 @@ int main(int argc, char **argv) {
   ops_par_loop(hc_zero_kernel, "hc_zero_kernel", g.blk, 2, fy1,
                ops_arg_dat(Ky, 1, g.S00, "double", OPS_WRITE));
   if (do64 && do32) ops_dat_deep_copy(x64, u64);
+  ops_dat Kx32 = nullptr, Ky32 = nullptr, r32 = nullptr, p32 = nullptr, w32 = nullptr;
   const double cells = (double)N * N;
   double t64 = 0.0, t32 = 0.0;
 
@@ -302,11 +305,11 @@ int main(int argc, char **argv) {
   }
 
   if (do32) {
-    ops_dat Kx32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "Kx32");
-    ops_dat Ky32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "Ky32");
-    ops_dat r32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "r32");
-    ops_dat p32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "p32");
-    ops_dat w32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "w32");
+    Kx32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "Kx32");
+    Ky32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "Ky32");
+    r32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "r32");
+    p32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "p32");
+    w32 = ops_decl_dat(g.blk, 1, size, base, d_m, d_p, nullf, "float", "w32");
     int all[] = {0, N + 1, 0, N + 1};
     ops_par_loop(hc_coef32_kernel, "hc_coef32_kernel", g.blk, 2, all,
                  ops_arg_dat(Kx32, 1, g.S00, "float", OPS_WRITE),
@@ -349,6 +352,12 @@ int main(int argc, char **argv) {
     free(hx);
     ops_printf("compare max_rel_diff %.15e\n", dmax / umax);
     ops_printf("timing ratio_fp64_over_mixed %.3f\n", t64 / t32);
+  }
+  const char *dump = sopt(argc, argv, "-dump=");
+  if (dump) {  // every dat through the public fetch call (apps/dumpdats.h)
+    ops_dat all[] = {den, b, Kx, Ky, u64, r, p, w, x64, Kx32, Ky32, r32, p32, w32};
+    if (dump_dats(dump, all, (int)(sizeof(all) / sizeof(all[0]))) != 0)
+      ops_printf("dump to %s failed\n", dump);
   }
   ops_timing_output(std::cout);
   ops_exit();

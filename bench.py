@@ -1,7 +1,7 @@
 """Benchmark: OPS 2D compressible hydro (CloverLeaf application) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--cells 3840] [--no-baseline]
+                    [--cells 3840] [--no-baseline] [--configs all|none|a,b]
 
 Workload: the CloverLeaf 2D Lagrangian-Eulerian hydro application, unchanged
 OPS user code, on 3840 x 3840 cells (ideal gas gamma=1.4, background rho=0.2
@@ -19,7 +19,10 @@ reference  the same app on the reference's own OpenMP backend (built from the
            reference sources), all host cores, rank 0 only.
 
 Prints one JSON line (rank 0).  value = cell updates per second over all
-ranks (GLUPS).
+ranks (GLUPS).  At N=1 the line also carries `configs`: the multi-block
+Poisson, 3D ADI, CG heat and solve-serving configurations, each run in its own
+process with its own clock record, HBM fraction and CPU baseline
+(apps/config_bench.py).
 """
 
 from __future__ import annotations
@@ -124,6 +127,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         os.unlink(self.path)
+        self.proc = None
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
@@ -273,40 +277,36 @@ def run_ours(a, d: Dist):
         report = buf.value.decode()
         B.ob2_ktime_enable(0)
 
-    # end to end through the C ABI: the hydro state (density0, energy0,
-    # xvel0, yvel0) comes in from pinned host buffers with ops_dat_set_data,
-    # K steps run, the same fields go back with ops_dat_fetch_data; host
-    # wall clock around all of it.
-    names = ["density0", "energy0", "xvel0", "yvel0"]
-    dats = [ctypes.c_void_p.in_dll(L, nm) for nm in names]
-    B.ops_dat_get_extents.argtypes = [ctypes.c_void_p, ctypes.c_int,
-                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
-    bufs, nbytes = [], 0
-    for dd in dats:
-        sz = (ctypes.c_int * 2)()
-        B.ops_dat_get_extents(dd, 0, None, sz)
-        nb = sz[0] * sz[1] * 8
+    # end to end through the C ABI: every dat of the application (the whole
+    # hydro state, work arrays and mesh included; interiors, 35 dats) comes in
+    # from pinned host buffers with ops_dat_set_data, K steps run, and every
+    # dat goes back with ops_dat_fetch_data; host wall clock around all of it.
+    L.clover_step_state.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    ndat = L.clover_step_state(0, None, None)
+    sizes = (ctypes.c_longlong * ndat)()
+    L.clover_step_state(0, None, sizes)
+    bufs = (ctypes.c_void_p * ndat)()
+    nbytes = 0
+    for i in range(ndat):
         p = ctypes.c_void_p()
-        B.ob2_host_alloc_pinned(ctypes.byref(p), ctypes.c_size_t(nb))
-        B.ops_dat_fetch_data.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
-        B.ops_dat_fetch_data(dd, 0, p)
-        bufs.append(p)
-        nbytes += nb
-    B.ops_dat_set_data.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        B.ob2_host_alloc_pinned(ctypes.byref(p), ctypes.c_size_t(sizes[i]))
+        bufs[i] = p.value
+        nbytes += sizes[i]
+    L.clover_step_state(0, bufs, None)  # current state into the host buffers
     B.ob2_dev_sync()
     d.barrier()
     t0 = time.perf_counter()
-    for dd, p in zip(dats, bufs):
-        B.ops_dat_set_data(dd, 0, p)
+    L.clover_step_state(1, bufs, None)
     L.clover_step_run(a.steps)
-    for dd, p in zip(dats, bufs):
-        B.ops_dat_fetch_data(dd, 0, p)
+    L.clover_step_state(0, bufs, None)
     e2e_s = d.max(time.perf_counter() - t0)
+    for i in range(ndat):
+        B.ob2_host_free_pinned(ctypes.c_void_p(bufs[i]))
     L.clover_step_summary()
     L.clover_step_finish()
     os.chdir(here)
     return {"t_ms": t_ms, "launches": launches, "report": report, "clocks": clk,
-            "e2e_s": e2e_s, "e2e_state_bytes": nbytes}
+            "e2e_s": e2e_s, "e2e_state_bytes": nbytes, "e2e_dats": ndat}
 
 
 def main(argv=None):
@@ -323,6 +323,10 @@ def main(argv=None):
     ap.add_argument("--baseline-steps", type=int, default=2)
     ap.add_argument("--report", action="store_true",
                     help="print the per-kernel device-time table to stderr")
+    ap.add_argument("--configs", default="all",
+                    help="the other configurations to add under 'configs' (N=1 only): "
+                         "all, none, or a comma list of poisson_2x2, adi_256, cg_heat_4096, "
+                         "serving")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         a.warmup = 3
@@ -346,7 +350,7 @@ def main(argv=None):
                 "warmup": a.warmup, "ms_per_step": r["s_per_step"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded input deck)", "impl": "reference",
-                "config": dict(config, parallelism="openmp %d threads" % cores),
+                "config": config, "parallelism": "openmp %d threads" % cores,
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                                  "sample": "%d steps after %d warm-up steps of the full config"
                                            % (a.steps, a.warmup)},
@@ -383,7 +387,11 @@ def main(argv=None):
             traffic = ncu_traffic().get(name)
             roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "algorithmic_bytes_per_launch": byts / cnt,
+                    "traffic": traffic,
+                    "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                                       "launch at this size, from the committed capture "
+                                       "profiles/ncu_traffic.txt (not measured in this run)"),
+                    "algorithmic_bytes_per_launch": byts / cnt,
                     "avg_launch_us": avg_s * 1e6, "share_of_device_time": dms / tot if tot else None}
             step_bytes = sum(r[3] for r in rows) / a.steps
             roof["step_algorithmic_GBps"] = step_bytes / (res["t_ms"] * 1e-3 / a.steps) / 1e9
@@ -400,17 +408,29 @@ def main(argv=None):
             except Exception as e:  # noqa: BLE001
                 base = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
                         "sample": "unavailable: " + str(e).splitlines()[-1][:160]}
+        configs = None
+        if d.world == 1 and a.configs != "none":
+            from apps import config_bench
+            names = (list(config_bench.CONFIGS) if a.configs == "all"
+                     else [c for c in a.configs.split(",") if c])
+            configs = config_bench.run_all(names, ClockSampler(d.local), peak, host_cores(),
+                                           baseline=not a.no_baseline)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": res["t_ms"] / a.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded input deck)",
-                "config": dict(config, parallelism="replicas x%d" % d.world),
+                "config": config, "parallelism": "replicas x%d" % d.world,
                 "roofline": roof, "cpu_baseline": base,
                 "e2e": {"value": e2e_v, "unit": UNIT,
                         "h2d_bytes_per_step": res["e2e_state_bytes"] / a.steps,
                         "d2h_bytes_per_step": res["e2e_state_bytes"] / a.steps,
-                        "note": "state in from and out to pinned host buffers around K steps"},
+                        "note": "all %d dats of the application (%.2f GB) set from pinned host "
+                                "buffers before and fetched back after the K steps "
+                                "(ops_dat_set_data / ops_dat_fetch_data)"
+                                % (res["e2e_dats"], res["e2e_state_bytes"] / 1e9)},
                 "gpu_launches": launches, "clocks": res["clocks"]}
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line), flush=True)
     d.close()
     return 0

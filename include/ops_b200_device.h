@@ -88,10 +88,19 @@ OB2_API int ob2_halo_run(const ob2_halo_task *tasks_dev, int ntasks, long long m
  * kernel itself is the same as ob2_halo_run's.
  *
  * - Returns OB2_ERR_NOALLOC_LIMIT (see ob2_error_string) when ntasks exceeds
- *   OB2_HALO_STATIC_MAX, without copying or launching anything.
+ *   OB2_HALO_STATIC_MAX, and cudaErrorInvalidValue when ntasks is negative
+ *   (or tasks_host is NULL with ntasks > 0), without copying or launching
+ *   anything.
+ * - Must be called with the device that ob2_dev_init selected current (the
+ *   work stream belongs to it); otherwise returns cudaErrorInvalidDevice.
  * - The first call on a device looks up the array's device address on that
  *   device (cudaGetSymbolAddress); make that first call before any stream
  *   capture begins.
+ * - The table is copied with cudaMemcpyAsync on the work stream.  From pinned
+ *   host memory that copy runs later, when the stream reaches it: keep the
+ *   caller's table unchanged until then (for example until ob2_dev_sync
+ *   returns).  From pageable memory the table is read before the call
+ *   returns.
  * - All calls share the one array, which keeps the last call's table: two
  *   calls whose work overlaps on the GPU (different streams, or different
  *   host threads) race on it.  Calls on one stream are ordered and safe.

@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "ops_b200_device.h"
 
@@ -17,6 +18,7 @@ namespace {
 cudaStream_t g_stream = nullptr;   // current work stream
 cudaStream_t g_default = nullptr;  // the runtime's own non-blocking stream
 int g_sms = 148;
+int g_device = -1;                 // the device ob2_dev_init selected
 
 inline int rc(cudaError_t e) { return (int)e; }
 
@@ -30,6 +32,7 @@ OB2_API int ob2_dev_init(int device) {
   if (device < 0 || device >= n) device = 0;
   e = cudaSetDevice(device);
   if (e != cudaSuccess) return rc(e);
+  g_device = device;
   cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, device);
   if (!g_default) {
     e = cudaStreamCreateWithFlags(&g_default, cudaStreamNonBlocking);
@@ -181,33 +184,40 @@ __device__ __align__(256) ob2_halo_task g_halo_static[OB2_HALO_STATIC_MAX];
 
 constexpr int kMaxDevices = 64;
 // device address of g_halo_static, looked up once per device (host code may
-// not pass the symbol itself to a kernel: its host-side name is a stand-in)
-ob2_halo_task *g_halo_static_addr[kMaxDevices] = {nullptr};
+// not pass the symbol itself to a kernel: its host-side name is a stand-in);
+// atomic so that first calls from several host threads do not race
+std::atomic<ob2_halo_task *> g_halo_static_addr[kMaxDevices];
 
 }  // namespace
 
 OB2_API int ob2_halo_run_noalloc(const ob2_halo_task *tasks_host, int ntasks) {
-  if (ntasks < 0 || ntasks > OB2_HALO_STATIC_MAX) return OB2_ERR_NOALLOC_LIMIT;
+  if (ntasks < 0 || (ntasks > 0 && !tasks_host)) return (int)cudaErrorInvalidValue;
+  if (ntasks > OB2_HALO_STATIC_MAX) return OB2_ERR_NOALLOC_LIMIT;
   if (ntasks == 0) return 0;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return rc(e);
   if (dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
-  if (!g_halo_static_addr[dev]) {
+  // the launch goes to the work stream, which belongs to the device that
+  // ob2_dev_init selected: the array looked up must be that device's
+  if (g_device >= 0 && dev != g_device) return (int)cudaErrorInvalidDevice;
+  ob2_halo_task *table = g_halo_static_addr[dev].load(std::memory_order_acquire);
+  if (!table) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_halo_static);
     if (e != cudaSuccess) return rc(e);
-    g_halo_static_addr[dev] = (ob2_halo_task *)p;
+    table = (ob2_halo_task *)p;
+    g_halo_static_addr[dev].store(table, std::memory_order_release);
   }
   long long max_pts = 0;
   for (int i = 0; i < ntasks; i++)
     if (tasks_host[i].npts > max_pts) max_pts = tasks_host[i].npts;
   // stream-ordered: an earlier launch on this stream still reading the table
   // finishes before it is overwritten
-  e = cudaMemcpyAsync(g_halo_static_addr[dev], tasks_host, sizeof(ob2_halo_task) * ntasks,
+  e = cudaMemcpyAsync(table, tasks_host, sizeof(ob2_halo_task) * ntasks,
                       cudaMemcpyHostToDevice, g_stream);
   if (e != cudaSuccess) return rc(e);
-  return ob2_halo_run(g_halo_static_addr[dev], ntasks, max_pts);
+  return ob2_halo_run(table, ntasks, max_pts);
 }
 
 // ---------------------------------------------------------------------------

@@ -1015,7 +1015,14 @@ OPS_API void ops_dat_deep_copy(ops_dat target, ops_dat src) {
   target->user_managed = 0;
   target->index = idx;
   target->block = blk;
-  target->name = copy_str(src->name);
+  // the copy is renamed to the source name + "_copy", cut to strlen(name) + 4
+  // characters as in ops_lib_core.cpp:2280-2281 (so "u" becomes "u_cop")
+  {
+    size_t nl = strlen(src->name) + 5;
+    char *nm = (char *)malloc(nl + 1);
+    snprintf(nm, nl, "%s_copy", src->name);
+    target->name = nm;
+  }
   target->type = copy_str(src->type);
   put_data(src);
   check(ob2_dev_d2d(target->data_d, src->data_d, src->mem), "deep copy");

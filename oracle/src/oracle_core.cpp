@@ -216,7 +216,14 @@ OPS_API void ops_dat_deep_copy(ops_dat target, ops_dat src) {
   target->index = idx;
   target->user_managed = um;
   target->block = blk ? blk : src->block;
-  target->name = copy_str(src->name);
+  // the copy is renamed to the source name + "_copy", cut to strlen(name) + 4
+  // characters as in ops_lib_core.cpp:2280-2281 (so "u" becomes "u_cop")
+  {
+    size_t nl = strlen(src->name) + 5;
+    char *nm = (char *)malloc(nl + 1);
+    snprintf(nm, nl, "%s_copy", src->name);
+    target->name = nm;
+  }
   target->type = copy_str(src->type);
   memcpy(target->data, src->data, src->mem);
 }

@@ -1,0 +1,107 @@
+"""Parity at the full configuration sizes: the b200 build of each
+configuration against a CPU build of the same program on the same seeded
+inputs, every dat compared element by element.
+
+* CloverLeaf 2D hydro, 3840^2 cells, 5 steps: this backend against the
+  reference's own OpenMP backend (its legacy translator and libops_seq, built
+  from the reference sources).  Every dat's interior is read through
+  ops_dat_fetch_data on both sides (apps/dumpdats.h); the field summary
+  (volume, mass, pressure, internal and kinetic energy sums) is compared too.
+* 3D ADI heat, 256^3, 3 steps, FP64 and FP32 storage: this backend against
+  the CPU oracle (the reference's tridiagonal solve lives in the external
+  tridsolver library, which the reference tree does not contain, so the
+  oracle's Thomas restatement is the checker for the solves).
+* CG heat conduction, 4096^2, 40 CG iterations (tolerance 0, so the count is
+  fixed) in the FP64 and the mixed form: this backend against the reference's
+  own sequential backend (ref_seq build of the driver), dats through
+  ops_dat_fetch_data.
+
+Tolerances: integer dats bit-exact; FP64 dats 1e-12 relative per element
+(|a-b| / max(|b|, 1e-3 max|b|)); FP32-stored dats 1e-6 (a float rounding of
+an FP64 value computed in another order); reductions 1e-11 relative.
+"""
+
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from tests.apprun import ROOT, assert_lines_close, ensure, result_lines, run_app
+from tests.opsdump import compare, read_dump
+
+pytestmark = pytest.mark.gpu
+
+
+def check(gpu_dump, cpu_dump, tol=1e-12, float_tol=1e-6):
+    diffs = compare(gpu_dump, cpu_dump, mmap=True)
+    meta = read_dump(cpu_dump, mmap=True)
+    bad = {n: d for n, d in diffs.items()
+           if d > (float_tol if meta[n][0]["type"] == "float" else tol)}
+    assert diffs and not bad, bad
+    return diffs
+
+
+def test_cloverleaf_3840_matches_reference_openmp(tmp_path):
+    ensure("clover_step", "b200")
+    ensure("clover_step", "ref_omp")
+    res, dumps = {}, {}
+    for fl in ("b200", "ref_omp"):
+        dumps[fl] = str(tmp_path / ("%s.dump" % fl))
+        r = subprocess.run([sys.executable, "-m", "apps.clover_run", "--flavour", fl, "--cells",
+                            "3840", "--steps", "5", "--fetch-dump", dumps[fl]], cwd=ROOT,
+                           capture_output=True, text=True, timeout=1200)
+        assert r.returncode == 0, r.stderr[-2000:]
+        res[fl] = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    try:
+        diffs = check(dumps["b200"], dumps["ref_omp"])
+        assert len(diffs) == 35
+    finally:
+        for p in dumps.values():
+            if os.path.exists(p):
+                os.unlink(p)
+    sg, sr = res["b200"]["summary"], res["ref_omp"]["summary"]
+    assert sg["step"] == sr["step"] == 5
+    for k in ("volume", "mass", "pressure", "ie", "ke"):
+        assert abs(sg[k] - sr[k]) <= 1e-11 * abs(sr[k]), (k, sg[k], sr[k])
+
+
+@pytest.mark.parametrize("prec", ["64", "32"])
+def test_adi_256_matches_oracle(prec, tmp_path):
+    args = ["-n=256", "-steps=3", "-prec=" + prec]
+    try:
+        gout, gd = run_app("adi3d", "b200", args, dump=True)
+        cout, cd = run_app("adi3d", "oracle", args, dump=True)
+        check(gd, cd)
+    finally:
+        for p in (locals().get("gd"), locals().get("cd")):
+            if p and os.path.exists(p):
+                os.unlink(p)
+    key = "fp64" if prec == "64" else "fp32"
+    g = [l for l in result_lines(gout, (key,)) if "checksum" in l]
+    c = [l for l in result_lines(cout, (key,)) if "checksum" in l]
+    assert_lines_close(g, c, 1e-11 if prec == "64" else 1e-6)
+
+
+@pytest.mark.parametrize("prec", ["64", "32"])
+def test_heat_cg_4096_matches_reference_seq(prec, tmp_path):
+    exe = ensure("heat_cg", "ref_seq", shared=False)
+    gd, cd = str(tmp_path / "b200.dump"), str(tmp_path / "ref.dump")
+    args = ["-n=4096", "-tol=0", "-maxit=40", "-prec=" + prec]
+    try:
+        gout, _ = run_app("heat_cg", "b200", args + ["-dump=" + gd])
+        r = subprocess.run([exe, *args, "-dump=" + cd], capture_output=True, text=True,
+                           timeout=1800)
+        assert r.returncode == 0, r.stderr[-2000:]
+        cout = r.stdout
+        check(gd, cd)
+    finally:
+        for p in (gd, cd):
+            if os.path.exists(p):
+                os.unlink(p)
+    key = "fp64" if prec == "64" else "mixed"
+    g = [l for l in result_lines(gout, (key,)) if "iterations" in l or "checksum" in l]
+    c = [l for l in result_lines(cout, (key,)) if "iterations" in l or "checksum" in l]
+    assert len(g) == 2, gout[-1000:]
+    assert_lines_close(g, c, 1e-11)

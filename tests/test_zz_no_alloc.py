@@ -3,9 +3,11 @@ device memory (their memory budget belongs to someone else, or they run where
 allocations are not allowed).  Its task table sits in a fixed array inside
 libops_b200.so instead of memory the caller allocates.
 
-Checked through the C ABI against ob2_halo_run (caller-allocated table) on
-the same inputs, on two calls in a row with different tables, and against its
-size limit.  Halo copies are exact, so the outputs must be identical.
+Checked through the C ABI against ob2_halo_run (caller-allocated table) and
+against the numpy model of the reference's halo semantics on the same inputs,
+on two calls in a row with different tables, with a table of exactly the
+maximum size, and against its error returns (a table above the maximum, a
+negative count).  Halo copies are exact, so the outputs must be identical.
 This file is collected last and also runs alone in a fresh process.
 """
 
@@ -113,6 +115,16 @@ def run_both(tasks, src, dst, s0, d0):
     return with_alloc, dst.get_full()
 
 
+def model(tasks_spec, src, dst, s0, d0):
+    """The numpy model of the reference's halo semantics applied task by task
+    (tests/test_gpu_cabi.py: np_halo)."""
+    from tests.test_gpu_cabi import np_halo
+    out = d0.copy()
+    for iters, fb, tb, fd, td in tasks_spec:
+        out = np_halo(s0, out, src.d_m, dst.d_m, iters, fb, tb, fd, td)
+    return out
+
+
 def test_noalloc_matches_allocating_entry_twice():
     from tests import cabi
     L = cabi.lib()
@@ -122,17 +134,42 @@ def test_noalloc_matches_allocating_entry_twice():
     rng = np.random.default_rng(11)
     s0 = rng.standard_normal(src.full_shape())
     d0 = rng.standard_normal(dst.full_shape())
-    first = [make_task(src, dst, 0, 0, [6, 4], [1, 2], [-2, -2], [-1, 2], [2, -1]),
-             make_task(src, dst, 0, 0, [1, 18], [23, 0], [-1, 0], [1, 2], [2, 1])]
+    spec1 = [([6, 4], [1, 2], [-2, -2], [-1, 2], [2, -1]),
+             ([1, 18], [23, 0], [-1, 0], [1, 2], [2, 1])]
+    first = [make_task(src, dst, 0, 0, *t) for t in spec1]
     a1, n1 = run_both(first, src, dst, s0, d0)
     assert np.array_equal(a1, n1)
+    assert np.array_equal(n1, model(spec1, src, dst, s0, d0))
     assert not np.array_equal(a1, d0)  # the halos really moved data
     # a second call with a different (smaller) table: nothing of the first
     # call's table may leak into it
-    second = [make_task(src, dst, 0, 0, [18, 2], [3, 0], [0, 30], [2, 1], [1, 2])]
+    spec2 = [([18, 2], [3, 0], [0, 30], [2, 1], [1, 2])]
+    second = [make_task(src, dst, 0, 0, *t) for t in spec2]
     a2, n2 = run_both(second, src, dst, s0, d0)
     assert np.array_equal(a2, n2)
+    assert np.array_equal(n2, model(spec2, src, dst, s0, d0))
     assert not np.array_equal(a2, a1)
+
+
+def test_noalloc_full_table_of_the_maximum_size():
+    """Exactly OB2_HALO_STATIC_MAX one-point tasks (the accepted upper edge):
+    point k of a 32 x 32 block of the source goes to the transposed point of
+    the target."""
+    from tests import cabi
+    L = cabi.lib()
+    b = L.ops_decl_block(2, b"noalloc_max")
+    src = cabi.Dat(b, 2, [32, 32], [0, 0], [0, 0], "double", "nm_src")
+    dst = cabi.Dat(b, 2, [32, 32], [0, 0], [0, 0], "double", "nm_dst")
+    rng = np.random.default_rng(5)
+    s0 = rng.standard_normal(src.full_shape())
+    d0 = rng.standard_normal(dst.full_shape())
+    spec = [([1, 1], [k % 32, k // 32], [k // 32, k % 32], [1, 2], [1, 2])
+            for k in range(OB2_HALO_STATIC_MAX)]
+    tasks = [make_task(src, dst, 0, 0, *t) for t in spec]
+    a, n = run_both(tasks, src, dst, s0, d0)
+    assert np.array_equal(a, n)
+    assert np.array_equal(n, s0.T)
+    assert np.array_equal(n, model(spec, src, dst, s0, d0))
 
 
 def test_noalloc_rejects_tables_above_the_limit():
@@ -145,3 +182,24 @@ def test_noalloc_rejects_tables_above_the_limit():
     assert rc == OB2_ERR_NOALLOC_LIMIT
     assert b"maximum" in L.ob2_error_string(rc)
     assert L.ob2_dev_sync() == 0
+
+
+def test_noalloc_rejects_a_negative_count_without_launching():
+    from tests import cabi
+    L = cabi.lib()
+    L.ob2_halo_run_noalloc.argtypes = [C.c_void_p, C.c_int]
+    L.ob2_error_string.restype = C.c_char_p
+    b = L.ops_decl_block(2, b"noalloc_neg")
+    src = cabi.Dat(b, 2, [8, 8], [0, 0], [0, 0], "double", "nn_src")
+    dst = cabi.Dat(b, 2, [8, 8], [0, 0], [0, 0], "double", "nn_dst")
+    d0 = np.arange(64, dtype=np.float64).reshape(8, 8)
+    src.set_full(-d0)
+    dst.set_full(d0)
+    t = make_task(src, dst, device_base(src), device_base(dst), [8, 8], [0, 0], [0, 0],
+                  [1, 2], [1, 2])
+    one = (HaloTask * 1)(t)
+    rc = L.ob2_halo_run_noalloc(one, -1)
+    assert rc == 1  # cudaErrorInvalidValue
+    assert b"maximum" not in L.ob2_error_string(rc)
+    assert L.ob2_dev_sync() == 0
+    assert np.array_equal(dst.get_full(), d0)  # nothing was copied
