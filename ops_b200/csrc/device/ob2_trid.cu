@@ -329,6 +329,151 @@ __global__ void __launch_bounds__(kThreads) trid_cta_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined persistent form of trid_cta_kernel (8-point chunks, P <= 32
+// chunks per line, LPB = 256 / P lines per work item).  Each CTA walks the
+// work items (groups of LPB lines) with a stride of the grid; while it
+// eliminates, reduces and substitutes one item, the coefficients of its next
+// item are already on their way into shared memory through asynchronous
+// copies (cp.async, 4- or 8-byte elements: no alignment demand beyond the
+// element's own).  Every thread copies exactly the elements it will consume
+// itself, so the staging needs no CTA barrier: cp.async.wait_all makes the
+// thread's own copies visible to it.  For the _Inc form u comes through a
+// second, double-buffered stage so that the next item's u can land while
+// this item's u is still being added to.  Two CTAs per SM keep about 128 KB
+// of loads in flight per SM, so the HBM stays busy through the FP64
+// divisions of the elimination and the barriers of the PCR.
+//
+// Mapping: LM (strided lines) puts consecutive threads on the same chunk of
+// neighbouring lines (contiguous along x: every copy of a warp is LPB-element
+// runs); !LM (unit-stride lines) puts the P chunks of a line on consecutive
+// threads.  The arithmetic per line is that of trid_cta_kernel.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_el(void *dst, const void *src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+constexpr int kPipeCL = 8;
+
+template <typename T, bool INC, bool LM>
+__global__ void __launch_bounds__(kThreads, 2) trid_pipe_kernel(
+    int n, int P, int LPB, long long nitems, long long nlines, long long stride, int o1n,
+    long long o1s, long long o2s, const T *__restrict__ A, const T *__restrict__ B,
+    const T *__restrict__ C, T *__restrict__ D, T *__restrict__ U) {
+  constexpr int CL = kPipeCL;
+  extern __shared__ double sm[];
+  const int tid = threadIdx.x;
+  const int p = LM ? tid / LPB : tid % P, l = LM ? tid % LPB : tid / P;
+  const bool mine = l < LPB && p < P;  // threads past LPB * P stay idle
+  const int m = 2 * P;
+  double *ra = sm + (size_t)(l < LPB ? l : 0) * (m * 3 + 1);
+  double *rc = ra + m;
+  double *rd = rc + m;
+  // stage: [array * CL + i][thread] (consecutive threads, consecutive words)
+  T *stage = (T *)(sm + (size_t)LPB * (m * 3 + 1));
+  T *ustage = stage + (size_t)4 * CL * kThreads;  // [buffer][i][thread], _Inc only
+  const int k0 = p * CL;
+
+  auto line_base = [&](long long item, long long &base) -> int {
+    const long long line = item * LPB + l;
+    if (!mine || line >= nlines) return 0;
+    base = (line % o1n) * o1s + (line / o1n) * o2s;
+    return max(0, min(CL, n - k0));
+  };
+  auto issue = [&](long long item, int ub) {
+    long long base = 0;
+    const int len = line_base(item, base);
+#pragma unroll
+    for (int i = 0; i < CL; i++)
+      if (i < len) {
+        const long long e = base + (long long)(k0 + i) * stride;
+        cp_async_el(stage + (size_t)(0 * CL + i) * kThreads + tid, A + e, sizeof(T));
+        cp_async_el(stage + (size_t)(1 * CL + i) * kThreads + tid, B + e, sizeof(T));
+        cp_async_el(stage + (size_t)(2 * CL + i) * kThreads + tid, C + e, sizeof(T));
+        cp_async_el(stage + (size_t)(3 * CL + i) * kThreads + tid, D + e, sizeof(T));
+        if (INC)
+          cp_async_el(ustage + (size_t)(ub * CL + i) * kThreads + tid, U + e, sizeof(T));
+      }
+    cp_async_commit();
+  };
+
+  long long item = blockIdx.x;
+  int ub = 0;
+  if (item < nitems) issue(item, ub);
+  for (; item < nitems; item += gridDim.x, ub ^= 1) {
+    cp_async_wait_all();
+    long long base = 0;
+    const int len = line_base(item, base);
+    double a[CL], b[CL], c[CL], d[CL];
+#pragma unroll
+    for (int i = 0; i < CL; i++) {
+      a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
+      if (i < len) {
+        a[i] = (k0 + i == 0) ? 0.0 : (double)stage[(size_t)(0 * CL + i) * kThreads + tid];
+        b[i] = (double)stage[(size_t)(1 * CL + i) * kThreads + tid];
+        c[i] = (k0 + i == n - 1) ? 0.0 : (double)stage[(size_t)(2 * CL + i) * kThreads + tid];
+        d[i] = (double)stage[(size_t)(3 * CL + i) * kThreads + tid];
+      }
+    }
+    // the next item's copies go into the slots just read (this thread's own)
+    if (item + gridDim.x < nitems) issue(item + gridDim.x, ub ^ 1);
+    chunk_reduce<CL>(a, b, c, d);
+    if (mine) {
+      ra[2 * p] = a[0]; rc[2 * p] = c[0]; rd[2 * p] = d[0];
+      ra[2 * p + 1] = a[CL - 1]; rc[2 * p + 1] = c[CL - 1]; rd[2 * p + 1] = d[CL - 1];
+    }
+    __syncthreads();
+    for (int s = 1; s < m; s <<= 1) {
+      double na[2], nc[2], nd[2];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int r = 2 * (mine ? p : 0) + q;
+        const double ar = ra[r], cr = rc[r], dr = rd[r];
+        double a1 = 0.0, c1 = 0.0, d1 = 0.0, a2 = 0.0, c2 = 0.0, d2 = 0.0;
+        const bool hl = r - s >= 0, hr = r + s < m;
+        if (hl) { a1 = ra[r - s]; c1 = rc[r - s]; d1 = rd[r - s]; }
+        if (hr) { a2 = ra[r + s]; c2 = rc[r + s]; d2 = rd[r + s]; }
+        const double k1l = hl ? ar : 0.0, k2r = hr ? cr : 0.0;
+        const double inv = 1.0 / (1.0 - k1l * c1 - k2r * a2);
+        na[q] = -k1l * a1 * inv;
+        nc[q] = -k2r * c2 * inv;
+        nd[q] = (dr - k1l * d1 - k2r * d2) * inv;
+      }
+      __syncthreads();
+      if (mine) {
+        ra[2 * p] = na[0]; rc[2 * p] = nc[0]; rd[2 * p] = nd[0];
+        ra[2 * p + 1] = na[1]; rc[2 * p + 1] = nc[1]; rd[2 * p + 1] = nd[1];
+      }
+      __syncthreads();
+    }
+    if (len > 0) {
+      const double xf = rd[2 * p], xl = rd[2 * p + 1];
+#pragma unroll
+      for (int i = 0; i < CL; i++)
+        if (i < len) {
+          const double x = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+          const long long e = base + (long long)(k0 + i) * stride;
+          if (INC)
+            U[e] = (T)((double)ustage[(size_t)(ub * CL + i) * kThreads + tid] + x);
+          else
+            D[e] = (T)x;
+        }
+    }
+    __syncthreads();  // the next item's end rows overwrite ra / rc / rd
+  }
+  cp_async_wait_all();
+}
+
 // Strided lines (y, z): one thread per line, neighbouring threads on
 // neighbouring lines along the fastest other axis, so every load and store
 // of a warp is one contiguous run.  The Thomas algorithm in FP64 with the
@@ -494,6 +639,49 @@ int launch_cta(const Lines &g, const void *a, const void *b, const void *c, void
   return (int)cudaGetLastError();
 }
 
+template <typename T, bool LM>
+int launch_pipe(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  constexpr int CL = kPipeCL;
+  const int P = (g.n + CL - 1) / CL;
+  if (P > 32) return (int)cudaErrorInvalidValue;
+  const int LPB = kThreads / P;
+  const long long nitems = (g.nlines + LPB - 1) / LPB;
+  const size_t pcr = (size_t)LPB * (2 * P * 3 + 1) * sizeof(double);
+  const size_t stage = (size_t)(4 + (u ? 2 : 0)) * CL * kThreads * sizeof(T);
+  const size_t shmem = pcr + stage;
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long grid = std::min(nitems, 2LL * sms);
+  if (u) {
+    cudaFuncSetAttribute(trid_pipe_kernel<T, true, LM>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    trid_pipe_kernel<T, true, LM><<<(unsigned)grid, kThreads, shmem, st>>>(
+        g.n, P, LPB, nitems, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a,
+        (const T *)b, (const T *)c, (T *)d, (T *)u);
+  } else {
+    cudaFuncSetAttribute(trid_pipe_kernel<T, false, LM>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    trid_pipe_kernel<T, false, LM><<<(unsigned)grid, kThreads, shmem, st>>>(
+        g.n, P, LPB, nitems, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, (const T *)a,
+        (const T *)b, (const T *)c, (T *)d, (T *)nullptr);
+  }
+  return (int)cudaGetLastError();
+}
+
+// OB2_TRID_PIPE: 1 (default) solves lines of 2 to 256 points with the
+// pipelined persistent kernel, for strided and unit-stride lines and both
+// element sizes; 0 keeps the kernels below.
+bool use_pipe(const Lines &g) {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("OB2_TRID_PIPE");
+    v = e ? atoi(e) : 1;
+  }
+  return v == 1 && g.n >= 2 && g.n <= 32 * kPipeCL;
+}
+
 // OB2_TRID_STRIDED: how strided lines are solved.  Measured on the 256^3
 // FP64 y / z solves (CUDA events, 20 steps): 3 the line-major CTA kernel
 // with 8-point chunks (8 lines x 32 chunks per CTA, 64-byte runs, 2 CTAs per
@@ -555,6 +743,10 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   g.unit = g.stride == 1 ? 1 : 0;
   if (g.n <= 0 || g.nlines <= 0) return 0;
   if (use_thomas(g.unit)) return launch_thomas<T>(g, a, b, c, d, u);
+  if (use_pipe(g)) {
+    if (g.unit) return launch_pipe<T, false>(g, a, b, c, d, u);
+    return launch_pipe<T, true>(g, a, b, c, d, u);
+  }
   switch (line_major_chunk<T>(g)) {
     case 8:
       return launch_cta<T, 8, true>(g, a, b, c, d, u);

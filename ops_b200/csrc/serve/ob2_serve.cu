@@ -6,14 +6,15 @@
 // grid of a few CTAs per SM walks the global unit index over all active
 // requests, finds the request by binary search in the prefix table, and works
 // on that request's tile.  One engine iteration:
-//   pois_pw       p' = r + beta p, w = A p', per-tile (p', w)
-//   scalars_a     alpha per Poisson request
-//   pois_xr       x += alpha p' (FP64), r -= alpha w, per-tile (r, r); or
-//                 the FP64 residual b - A x
+//   pois_pass     one pass of the single-reduction CG over every Poisson /
+//                 heat request: the iteration (p, s, x, r and w = A r with
+//                 per-tile (r, r), (w, r)), or the FP64 residual b - A x and
+//                 w = A r of a residual replacement
 //   adi_pre       right-hand side of the ADI step (adi/preproc_kernel.h)
 //   adi_x/y/z     constant-coefficient Thomas solves (z adds into u)
-//   scalars_b     per request: fixed-order sum of its tile partials, beta,
-//                 residual replacement and convergence; ADI step count
+//   scalars_b     per request: fixed-order sum of its tile partials, alpha,
+//                 beta, residual replacement and convergence; heat time
+//                 steps; ADI step count
 // All kernels read the work list from device memory, so one captured graph
 // of K iterations serves every batch composition.
 #include <cuda_runtime.h>
@@ -34,16 +35,20 @@ constexpr int MAXA = OB2S_MAX_ACTIVE;
 constexpr int ADI_MAX_N = 192;  // x-solve tile: 32 lines x n points in shared memory
 constexpr int ADI_XL = 32;      // lines per x-solve unit
 constexpr int ADI_YZ = 4;       // planes per y/z-solve unit (CTA 32 x 4 lines)
+constexpr double kHeatRho = 1.0;  // heat requests: dt / h^2 of the implicit step
 
 struct Req {
   int kind, n, pitch, tiles_x, tiles;
   int phase, done, outer, inner_it, iters;
   int max_inner, max_outer, steps, step;
   int par;  // p buffer parity
+  int newstep;  // heat: the next pass starts a time step (b = x)
   double tol, inner_tol;
   double alpha, beta, gamma, gamma_in0, rr0, rel;
+  double diag, off;  // operator: diag x - off (sum of the 4 neighbours)
   double *x, *b, *part;
-  void *r, *w, *p0, *p1;
+  void *r[2], *w[2], *s[2], *p;
+  void *y;  // mixed mode: FP32 correction accumulator (NULL in FP64 mode)
   double *u, *du, *cp, *mm;
   double a_coef, lambda;
 };
@@ -83,32 +88,56 @@ __device__ __forceinline__ double hash_uniform(int seed, int i, int j, int k) {
 
 // ---------------------------------------------------------------- Poisson
 // CTA 32 x 8 threads; each thread handles RY consecutive rows, so a tile is
-// 32 x (8 RY) points.  Loads of out-of-range rows are clamped to the last
-// interior row (always valid memory) and only the stores are guarded, so the
-// loads of all RY rows are issued before any store.
+// 32 x (8 RY) points.  Loads of out-of-range rows are clamped to the zero
+// halo row below the grid (always valid memory) and only the stores are
+// guarded, so the loads of all rows are issued before any store.
 //
-// Poisson requests: conjugate gradients (the standard two-reduction form)
-// with the iterate x in FP64, the vectors r, w, p in TI (FP32 in the mixed
-// mode, FP64 otherwise) and every dot product accumulated in FP64.  The
-// recursive residual is replaced by the true one, b - A x computed in FP64,
-// whenever it has dropped by inner_tol since the last true residual or meets
-// the tolerance (reliable updates: the search direction is kept, so the
-// Krylov convergence of FP64 CG is kept too; an FP32 iterate or FP32
-// accumulation of x would instead stall far above 1e-8 on fine grids).
+// Poisson and heat requests: A x = diag x - off (sum of the 4 neighbours)
+// with a zero Dirichlet boundary (Poisson: diag 4, off 1; a backward-Euler
+// heat step: diag 1 + 4 rho, off rho), solved by conjugate gradients in the
+// single-reduction form of Chronopoulos and Gear ("s-step iterative methods
+// for symmetric linear systems", J. Comput. Appl. Math. 25, 1989): with
+// w = A r and s = A p carried along,
+//   p_i = r_i + beta_i p_{i-1}      s_i = w_i + beta_i s_{i-1}
+//   x_{i+1} = x_i + alpha_i p_i     r_{i+1} = r_i - alpha_i s_i
+//   w_{i+1} = A r_{i+1}             gamma = (r, r), delta = (w, r) at i+1
+//   beta_{i+1} = gamma_{i+1} / gamma_i
+//   alpha_{i+1} = gamma_{i+1} / (delta_{i+1} - beta_{i+1} gamma_{i+1} / alpha_i)
+// so that one pass over the vectors and one scalar kernel make an
+// iteration (the two-reduction form needs two passes and two scalar
+// kernels).  w_{i+1} needs r_{i+1} at the four neighbours: each thread forms
+// r_{i+1} = r_i - alpha (w_i + beta s_{i-1}) of its rows and of the rows above
+// and below itself, the warp's lanes exchange theirs by shuffles and the edge
+// lanes form their outer neighbours from memory with the same arithmetic, so
+// every value of r_{i+1} is computed identically wherever it is used.
+// r, w and s are double-buffered (read [par], written [par ^ 1]); p and the
+// iterate are updated in place (read only at their own point).
+//
+// Precision: the vectors r, w, s, p are stored in TI (FP32 in the mixed mode,
+// FP64 otherwise); every value is formed in FP64 from its stored inputs and
+// rounded once to TI; dot products accumulate in FP64.  The FP64 mode updates
+// the FP64 iterate x every iteration.  The mixed mode accumulates alpha p into
+// an FP32 correction y instead and folds y into the FP64 x at each residual
+// replacement (reliable updates with a low-precision accumulator, as in
+// mixed-precision Krylov solvers since Sleijpen and van der Vorst,
+// Computing 56, 1996): between replacements y holds only the correction since
+// the last fold, so its rounding shrinks with the error it corrects.  Per
+// point per iteration the mixed mode moves 40 bytes (r, w, s, p, y read and
+// written in FP32), the FP64 mode 80.
+// The recursive residual is replaced by b - A x computed in FP64 whenever it
+// has dropped by inner_tol since the last true residual or meets the
+// tolerance; the search directions p, s are kept.
 // Phases:
-//   0  start (and restart after a breakdown): r = b - A x in FP64
-//   2  CG iteration: p' = r + beta p, w = A p', (p', w)   [pois_pw]
-//                    alpha = gamma / (p', w)               [scalars_a]
-//                    x += alpha p', r -= alpha w, (r, r)   [pois_xr]
-//                    beta, gamma; replacement test         [scalars_b]
-//   3  replacement: r = b - A x in FP64, convergence test on it; beta from
-//      the true (r, r), p kept
-// p is double-buffered (p[par] read, p[par ^ 1] written by pois_pw), since
-// pois_pw forms p' of the stencil neighbours itself: w = A p' needs p' at
-// the neighbours, and recomputing r + beta p there avoids a separate pass.
+//   0  start (and restart after a breakdown; for heat requests also the start
+//      of each time step, which first sets b = x): r = b - A (x + y) [pois_pass]
+//   4  w = A r, fold x += y, y = 0, (r, r), (w, r)   [pois_pass]; alpha_0
+//   2  CG iteration                                  [pois_pass]; alpha, beta
+//   3  replacement: r = b - A (x + y) in FP64        [pois_pass]
+//   5  as 4, then beta from the true (r, r), p and s kept
+// The scalar kernel (scalars_b) moves every request to its next phase.
 
 constexpr int CTA_Y = 8;
-constexpr int NPART = 2;  // partial sums per tile: (p', w) and (r, r)
+constexpr int NPART = 2;  // partial sums per tile: (r, r) and (w, r)
 
 // resident CTAs per SM the Poisson kernels are compiled for (register cap)
 #ifndef OB2S_MINB
@@ -139,150 +168,174 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[32]) {
   __syncthreads();
 }
 
-// p' = r + beta p and w = A p' over the tile, (p', w) per tile (phase 2)
-template <typename TI, int RY>
-__global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[1][32];
-  const long long total = W->pois_pref[W->npois];
-  for (long long un = blockIdx.x; un < total; un += gridDim.x) {
-    const int k = find_req(W->pois_pref, W->npois, un);
-    const Req &q = R[W->pois_slot[k]];
-    if (q.done || q.phase != 2) continue;  // uniform over the CTA
-    const int t = (int)(un - W->pois_pref[k]);
-    const int n = q.n, P = q.pitch;
-    const int i = (t % q.tiles_x) * TX + threadIdx.x;
-    const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
-    double v[1] = {0.0};
-    if (j0 < n) {  // uniform over the warp (one threadIdx.y per warp)
-      const TI *rr = (const TI *)q.r;
-      const TI *pin = (const TI *)(q.par ? q.p1 : q.p0);
-      TI *pout = (TI *)(q.par ? q.p0 : q.p1);
-      TI *ww = (TI *)q.w;
-      const TI beta = (TI)q.beta;
-      const bool inx = i < n;
-      const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
-      const int lane = threadIdx.x;
-      // p' = r + beta p on rows j0-1 .. j0+RY of column i (storage rows
-      // clamped into the array; the halo rows and columns of r and p hold
-      // zeros); a lane past the right edge stands for the zero halo column
-      TI pc[RY + 2];
-      int o[RY + 2];  // (n + 2)^2 < 2^31 for n <= 32768
-#pragma unroll
-      for (int m = 0; m < RY + 2; m++) {
-        o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
-        pc[m] = inx ? rr[o[m]] + beta * pin[o[m]] : (TI)0;
-      }
-#pragma unroll
-      for (int m = 0; m < RY; m++) {
-        // west / east neighbours from the adjacent lanes; the warp's edge
-        // lanes form theirs from memory (the same arithmetic, same bits)
-        TI pw = __shfl_up_sync(0xffffffffu, pc[m + 1], 1);
-        TI pe = __shfl_down_sync(0xffffffffu, pc[m + 1], 1);
-        if (lane == 0) pw = rr[o[m + 1] - 1] + beta * pin[o[m + 1] - 1];
-        if (lane == TX - 1 && inx) pe = rr[o[m + 1] + 1] + beta * pin[o[m + 1] + 1];
-        if (!inx || j0 + m >= n) continue;
-        const TI c = pc[m + 1];
-        const TI a = (TI)4 * c - pw - pe - pc[m] - pc[m + 2];
-        pout[o[m + 1]] = c;
-        ww[o[m + 1]] = a;
-        v[0] += (double)c * (double)a;
-      }
-    }
-    block_sum<1>(v, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) q.part[NPART * t] = v[0];
-  }
+// r_{i+1} at one point from the stored r_i, w_i, s_{i-1}: the one expression
+// every thread uses for it
+template <typename TI>
+__device__ __forceinline__ TI next_r(TI r, TI w, TI s, double alpha, double beta, TI &s_new) {
+  s_new = (TI)((double)w + beta * (double)s);
+  return (TI)((double)r - alpha * (double)s_new);
 }
 
-// phase 2: x += alpha p', r -= alpha w, (r, r); phases 0, 3: r = b - A x in
-// FP64 and its (r, r)
+// one pass of a Poisson / heat request's current phase over the tile
 template <typename TI, int RY>
-__global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[1][32];
+__global__ void POIS_BOUNDS pois_pass(const Work *__restrict__ W, Req *R) {
+  __shared__ double sh[NPART][32];
   const long long total = W->pois_pref[W->npois];
+  const unsigned full = 0xffffffffu;
   for (long long un = blockIdx.x; un < total; un += gridDim.x) {
     const int k = find_req(W->pois_pref, W->npois, un);
     const Req &q = R[W->pois_slot[k]];
-    if (q.done) continue;  // uniform over the CTA
     const int ph = q.phase;
+    if (q.done) continue;  // uniform over the CTA
     const int t = (int)(un - W->pois_pref[k]);
     const int n = q.n, P = q.pitch;
-    const int i = (t % q.tiles_x) * TX + threadIdx.x;
+    const int lane = threadIdx.x;
+    const int i = (t % q.tiles_x) * TX + lane;
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
-    double v[1] = {0.0};
-    if (i < n && j0 < n) {
-      int o[RY];  // (n + 2)^2 < 2^31 for n <= 32768
+    const bool inx = i < n;
+    const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
+    const double diag = q.diag, off = q.off;
+    const int cur = q.par, nxt = q.par ^ 1;
+    const bool mixed = q.y != nullptr;
+    double v[NPART] = {0.0, 0.0};
+    if (j0 < n) {  // uniform over the warp (one threadIdx.y per warp)
+      // storage offsets of rows j0-1 .. j0+RY of column i, clamped into the
+      // array ((n + 2)^2 < 2^31 for n <= 32768)
+      int o[RY + 2];
 #pragma unroll
-      for (int m = 0; m < RY; m++) o[m] = (min(j0 + m, n - 1) + 1) * P + (i + 1);
-      TI *rr = (TI *)q.r;
-      double *x = q.x;
+      for (int m = 0; m < RY + 2; m++) o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
       if (ph == 2) {
-        const TI *pn = (const TI *)(q.par ? q.p0 : q.p1);  // written by pois_pw
-        const TI *ww = (const TI *)q.w;
-        const double alpha64 = q.alpha;
-        const TI alpha = (TI)q.alpha;
-        double xv[RY];
-        TI rv[RY];
+        const TI *r = (const TI *)q.r[cur], *w = (const TI *)q.w[cur];
+        const TI *s = (const TI *)q.s[cur];
+        TI *r1 = (TI *)q.r[nxt], *w1 = (TI *)q.w[nxt], *s1 = (TI *)q.s[nxt];
+        TI *pp = (TI *)q.p;
+        const double alpha = q.alpha, beta = q.beta;
+        TI rn[RY + 2], sn[RY + 2];
 #pragma unroll
-        for (int m = 0; m < RY; m++) {
-          const TI pv = pn[o[m]];
-          xv[m] = x[o[m]] + alpha64 * (double)pv;
-          rv[m] = rr[o[m]] - alpha * ww[o[m]];
+        for (int m = 0; m < RY + 2; m++) {
+          rn[m] = (TI)0;
+          sn[m] = (TI)0;
+          if (inx) rn[m] = next_r<TI>(r[o[m]], w[o[m]], s[o[m]], alpha, beta, sn[m]);
         }
 #pragma unroll
         for (int m = 0; m < RY; m++) {
-          if (j0 + m >= n) continue;
-          x[o[m]] = xv[m];
-          rr[o[m]] = rv[m];
-          v[0] += (double)rv[m] * (double)rv[m];
+          const int oc = o[m + 1];
+          TI rw = __shfl_up_sync(full, rn[m + 1], 1);
+          TI re = __shfl_down_sync(full, rn[m + 1], 1);
+          TI dummy;
+          if (lane == 0) rw = next_r<TI>(r[oc - 1], w[oc - 1], s[oc - 1], alpha, beta, dummy);
+          if (lane == TX - 1 && inx)
+            re = next_r<TI>(r[oc + 1], w[oc + 1], s[oc + 1], alpha, beta, dummy);
+          if (!inx || j0 + m >= n) continue;
+          const TI rc = rn[m + 1];
+          const TI wn = (TI)(diag * (double)rc -
+                             off * ((double)rw + (double)re + (double)rn[m] + (double)rn[m + 2]));
+          const TI pn = (TI)((double)r[oc] + beta * (double)pp[oc]);
+          if (mixed) {
+            TI *y = (TI *)q.y;
+            y[oc] = (TI)((double)y[oc] + alpha * (double)pn);
+          } else {
+            q.x[oc] = q.x[oc] + alpha * (double)pn;
+          }
+          pp[oc] = pn;
+          r1[oc] = rc;
+          s1[oc] = sn[m + 1];
+          w1[oc] = wn;
+          v[0] += (double)rc * (double)rc;
+          v[1] += (double)wn * (double)rc;
         }
-      } else {
-        const double *b = q.b;
-        double res[RY];
+      } else if (ph == 0 || ph == 3) {
+        // r = b - A (x + y) in FP64 (heat: b = x first at a new time step)
+        const double *x = q.x;
+        const TI *y = (const TI *)q.y;
+        double xs[RY + 2];
 #pragma unroll
-        for (int m = 0; m < RY; m++)
-          res[m] = b[o[m]] -
-                   (4.0 * x[o[m]] - x[o[m] - 1] - x[o[m] + 1] - x[o[m] - P] - x[o[m] + P]);
+        for (int m = 0; m < RY + 2; m++)
+          xs[m] = inx ? x[o[m]] + (mixed ? (double)y[o[m]] : 0.0) : 0.0;
+        TI *r = (TI *)q.r[cur];
 #pragma unroll
         for (int m = 0; m < RY; m++) {
-          if (j0 + m >= n) continue;
-          rr[o[m]] = (TI)res[m];
-          v[0] += res[m] * res[m];
+          const int oc = o[m + 1];
+          double xw = __shfl_up_sync(full, xs[m + 1], 1);
+          double xe = __shfl_down_sync(full, xs[m + 1], 1);
+          if (lane == 0) xw = x[oc - 1] + (mixed ? (double)y[oc - 1] : 0.0);
+          if (lane == TX - 1 && inx) xe = x[oc + 1] + (mixed ? (double)y[oc + 1] : 0.0);
+          if (!inx || j0 + m >= n) continue;
+          double bv = q.b[oc];
+          if (q.newstep) {
+            bv = xs[m + 1];
+            q.b[oc] = bv;
+          }
+          const double ax = diag * xs[m + 1] - off * (xw + xe + xs[m] + xs[m + 2]);
+          r[oc] = (TI)(bv - ax);
+        }
+      } else {  // phases 4, 5: w = A r, fold the correction, (r, r), (w, r)
+        const TI *r = (const TI *)q.r[cur];
+        TI *w = (TI *)q.w[cur];
+        TI rs[RY + 2];
+#pragma unroll
+        for (int m = 0; m < RY + 2; m++) rs[m] = inx ? r[o[m]] : (TI)0;
+#pragma unroll
+        for (int m = 0; m < RY; m++) {
+          const int oc = o[m + 1];
+          TI rw = __shfl_up_sync(full, rs[m + 1], 1);
+          TI re = __shfl_down_sync(full, rs[m + 1], 1);
+          if (lane == 0) rw = r[oc - 1];
+          if (lane == TX - 1 && inx) re = r[oc + 1];
+          if (!inx || j0 + m >= n) continue;
+          const TI rc = rs[m + 1];
+          const TI wn = (TI)(diag * (double)rc -
+                             off * ((double)rw + (double)re + (double)rs[m] + (double)rs[m + 2]));
+          w[oc] = wn;
+          if (mixed) {
+            TI *y = (TI *)q.y;
+            q.x[oc] = q.x[oc] + (double)y[oc];
+            y[oc] = (TI)0;
+          }
+          v[0] += (double)rc * (double)rc;
+          v[1] += (double)wn * (double)rc;
         }
       }
     }
-    block_sum<1>(v, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) q.part[NPART * t + 1] = v[0];
+    if (ph == 2 || ph == 4 || ph == 5) {  // uniform over the CTA
+      block_sum<NPART>(v, sh);
+      if (threadIdx.x == 0 && threadIdx.y == 0) {
+        q.part[NPART * t] = v[0];
+        q.part[NPART * t + 1] = v[1];
+      }
+    }
   }
 }
 
-// per-request fixed-order sum of one partial column
-__device__ __forceinline__ double request_sum(const Req &q, int col, double (*sh)[32]) {
-  double v[1] = {0.0};
-  for (int t = threadIdx.x; t < q.tiles; t += blockDim.x) v[0] += q.part[NPART * t + col];
-  block_sum<1>(v, sh);
-  return v[0];
+// per-request fixed-order sums of the two partial columns
+__device__ __forceinline__ void request_sums(const Req &q, double (*sh)[32], double &g,
+                                             double &d) {
+  double v[NPART] = {0.0, 0.0};
+  for (int t = threadIdx.x; t < q.tiles; t += blockDim.x) {
+    v[0] += q.part[NPART * t];
+    v[1] += q.part[NPART * t + 1];
+  }
+  block_sum<NPART>(v, sh);
+  g = v[0];
+  d = v[1];
 }
 
-// alpha = gamma / (p', w) for requests in phase 2
-__global__ void __launch_bounds__(256) scalars_a(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[1][32];
-  const int b = blockIdx.x;
-  if (b >= W->npois) return;
-  Req &q = R[W->pois_slot[b]];
-  if (q.done || q.phase != 2) return;
-  const double pw = request_sum(q, 0, sh);
-  if (threadIdx.x != 0) return;
-  if (!(pw > 0.0)) {  // breakdown: pois_xr computes the true residual and
-    q.phase = 0;       // scalars_b restarts from it with beta = 0
+// after a converged solve: the next heat time step, or done
+__device__ __forceinline__ void finish_solve(Req &q) {
+  if (q.kind == OB2S_HEAT2D && q.step + 1 < q.steps) {
+    q.step++;
+    q.newstep = 1;
+    q.outer = 0;
+    q.phase = 0;
     return;
   }
-  q.alpha = q.gamma / pw;
+  q.done = 1;
 }
 
-// (r, r) step of every Poisson request; CTAs [MAXA, MAXA + nadi) advance
-// the ADI requests' step counts
+// Every request's next phase (thread 0 of one CTA per request slot; CTAs
+// [MAXA, MAXA + nadi) advance the ADI requests' step counts).
 __global__ void __launch_bounds__(256) scalars_b(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[1][32];
+  __shared__ double sh[NPART][32];
   const int b = blockIdx.x;
   if (b >= MAXA) {
     const int k = b - MAXA;
@@ -297,32 +350,58 @@ __global__ void __launch_bounds__(256) scalars_b(const Work *__restrict__ W, Req
   if (b >= W->npois) return;
   Req &q = R[W->pois_slot[b]];
   if (q.done) return;
-  const double g = request_sum(q, 1, sh);
-  if (threadIdx.x != 0) return;
   const int ph = q.phase;
-  if (ph == 0 || ph == 3) {  // g = (b - A x, b - A x) in FP64
+  if (ph == 0 || ph == 3) {  // r written; w, the fold and the dots next
+    if (threadIdx.x == 0) {
+      q.newstep = 0;
+      q.phase = ph == 0 ? 4 : 5;
+    }
+    return;
+  }
+  double g, dl;
+  request_sums(q, sh, g, dl);
+  if (threadIdx.x != 0) return;
+  if (ph == 4 || ph == 5) {  // true residual: g = (r, r), dl = (w, r)
     if (q.outer == 0) q.rr0 = g;
     q.outer++;
     q.rel = q.rr0 > 0.0 ? sqrt(g / q.rr0) : 0.0;
-    if (q.rel <= q.tol || q.outer > q.max_outer || q.iters >= q.max_inner) {
-      q.done = 1;
+    if (q.rel <= q.tol || q.outer > q.max_outer || q.iters >= q.max_inner || g == 0.0) {
+      finish_solve(q);
       return;
     }
-    q.beta = ph == 0 ? 0.0 : g / q.gamma;
+    double beta = 0.0, den = dl;
+    if (ph == 5) {
+      beta = g / q.gamma;
+      den = dl - beta * g / q.alpha;
+    }
+    if (!(den > 0.0)) {  // breakdown: start again from the true residual
+      q.phase = 0;
+      return;
+    }
+    q.beta = beta;
+    q.alpha = g / den;
     q.gamma = g;
     q.gamma_in0 = g;
     q.phase = 2;
     return;
   }
+  // phase 2: recursive (r, r) and (w, r) of the new residual
   q.iters++;
   q.par ^= 1;
   const double drop = sqrt(g / q.gamma_in0);
   const double relr = q.rr0 > 0.0 ? sqrt(g / q.rr0) : 0.0;
   if (drop <= q.inner_tol || relr <= q.tol || q.iters >= q.max_inner || g == 0.0) {
-    q.phase = 3;  // gamma stays the previous (r, r) for beta
+    q.phase = 3;  // gamma and alpha stay those of the step just taken
     return;
   }
-  q.beta = g / q.gamma;
+  const double beta = g / q.gamma;
+  const double den = dl - beta * g / q.alpha;
+  if (!(den > 0.0)) {
+    q.phase = 3;  // loss of positivity: replace the residual and go on from it
+    return;
+  }
+  q.beta = beta;
+  q.alpha = g / den;
   q.gamma = g;
 }
 
@@ -449,6 +528,15 @@ __global__ void pois_init(double *b, int n, int pitch, int seed) {
   b[(long long)(j + 1) * pitch + i + 1] = h * h * (2.0 * hash_uniform(seed, i, j, 0) - 1.0);
 }
 
+// heat request: u0 ~ U(-1,1) into b and x
+__global__ void heat_init(double *b, double *x, int n, int pitch, int seed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= n) return;
+  const double v = 2.0 * hash_uniform(seed, i, j, 3) - 1.0;
+  b[(long long)(j + 1) * pitch + i + 1] = v;
+  x[(long long)(j + 1) * pitch + i + 1] = v;
+}
+
 __global__ void adi_init(double *u, int n, int seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, z = blockIdx.z;
   if (i >= n) return;
@@ -494,10 +582,12 @@ static int rc(cudaError_t e) { return (int)e; }
 static size_t elem_inner(int mode) { return mode == OB2S_MIXED ? 4 : 8; }
 
 OB2_API size_t ob2s_request_bytes(int mode, int kind, int n) {
-  if (kind == OB2S_POISSON2D) {
+  if (kind == OB2S_POISSON2D || kind == OB2S_HEAT2D) {
     const size_t p = (size_t)(n + 2) * (n + 2);
     const size_t tiles = (size_t)((n + 31) / 32) * (size_t)((n + 7) / 8);  // at the smallest tile
-    return p * (16 + 4 * elem_inner(mode)) + 8 * NPART * tiles + 4096;
+    // x, b (FP64); r, w, s (two buffers each) and p; y in the mixed mode
+    const size_t vec = 7 + (mode == OB2S_MIXED ? 1 : 0);
+    return p * (16 + vec * elem_inner(mode)) + 8 * NPART * tiles + 4096;
   }
   return (size_t)n * n * n * 16 + (size_t)n * 16 + 4096;
 }
@@ -509,10 +599,8 @@ static int launch_iteration(ob2s_engine *e, int variant) {
   int k = 0;
   if (variant & 1) {
     const int g = e->sms * e->pois_ctas_per_sm;
-    pois_pw<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
-    scalars_a<<<MAXA, 256, 0, e->st>>>(e->W_d, e->R_d);
-    pois_xr<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
-    k += 3;
+    pois_pass<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
+    k += 1;
   }
   if (variant & 2) {
     adi_pre<<<e->sms * 8, dim3(32, 8), 0, e->st>>>(e->W_d, e->R_d);
@@ -566,7 +654,7 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
   }
   {
     // persistent grids: as many CTAs as can be resident at once
-    int nb = 0, nb2 = 0;
+    int nb = 0;
     const bool mixed = mode == OB2S_MIXED;
     auto occ = [&](const void *f) {
       int b = 0;
@@ -575,17 +663,15 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
     };
     switch (tile_y) {
       case 8:
-        nb = occ(mixed ? (const void *)pois_pw<float, 1> : (const void *)pois_pw<double, 1>);
-        nb2 = occ(mixed ? (const void *)pois_xr<float, 1> : (const void *)pois_xr<double, 1>);
+        nb = occ(mixed ? (const void *)pois_pass<float, 1> : (const void *)pois_pass<double, 1>);
         break;
       case 16:
-        nb = occ(mixed ? (const void *)pois_pw<float, 2> : (const void *)pois_pw<double, 2>);
-        nb2 = occ(mixed ? (const void *)pois_xr<float, 2> : (const void *)pois_xr<double, 2>);
+        nb = occ(mixed ? (const void *)pois_pass<float, 2> : (const void *)pois_pass<double, 2>);
         break;
       default:
-        nb = occ(mixed ? (const void *)pois_pw<float, 4> : (const void *)pois_pw<double, 4>);
-        nb2 = occ(mixed ? (const void *)pois_xr<float, 4> : (const void *)pois_xr<double, 4>);
+        nb = occ(mixed ? (const void *)pois_pass<float, 4> : (const void *)pois_pass<double, 4>);
     }
+    const int nb2 = nb;
     e->pois_ctas_per_sm = std::max(1, std::min(nb, nb2));
   }
   e->R.assign(MAXA, Req());
@@ -633,8 +719,9 @@ static void host_thomas_coefs(int n, double lambda, std::vector<double> &cp,
 }
 
 OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, int *id) {
-  if (kind == OB2S_POISSON2D ? (n < 1 || n > 32768) : (kind != OB2S_ADI3D || n < 3 ||
-                                                       n > ADI_MAX_N || steps < 1))
+  const bool grid2d = kind == OB2S_POISSON2D || kind == OB2S_HEAT2D;
+  if (grid2d ? (n < 1 || n > 32768 || (kind == OB2S_HEAT2D && steps < 1))
+             : (kind != OB2S_ADI3D || n < 3 || n > ADI_MAX_N || steps < 1))
     return OB2S_ERR_BADARG;
   int slot = -1;
   for (int k = 0; k < MAXA; k++)
@@ -661,21 +748,32 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
     c += (b + 255) / 256 * 256;
     return (void *)p;
   };
-  if (kind == OB2S_POISSON2D) {
+  if (grid2d) {
     q.pitch = n + 2;
     q.tiles_x = (n + TX - 1) / TX;
     q.tiles = q.tiles_x * ((n + e->tile_y - 1) / e->tile_y);
     const size_t p = (size_t)q.pitch * q.pitch;
     const size_t ei = elem_inner(e->mode);
-    // the layout ob2s_request_bytes counts (seven arrays, each rounded up to
-    // 256 bytes: within its 4 KB slack)
+    // the layout ob2s_request_bytes counts (each array rounded up to 256
+    // bytes: within its 4 KB slack); every array starts zeroed
     q.x = (double *)take(p * 8);
     q.b = (double *)take(p * 8);
-    q.r = take(p * ei);
-    q.w = take(p * ei);
-    q.p0 = take(p * ei);
-    q.p1 = take(p * ei);
+    for (int c = 0; c < 2; c++) {
+      q.r[c] = take(p * ei);
+      q.w[c] = take(p * ei);
+      q.s[c] = take(p * ei);
+    }
+    q.p = take(p * ei);
+    q.y = e->mode == OB2S_MIXED ? take(p * ei) : nullptr;
     q.part = (double *)take((size_t)8 * NPART * q.tiles);
+    if (kind == OB2S_HEAT2D) {  // backward Euler, dt = h^2: (1 + 4) x - (neighbours)
+      q.diag = 1.0 + 4.0 * kHeatRho;
+      q.off = kHeatRho;
+      q.steps = steps;
+    } else {
+      q.diag = 4.0;
+      q.off = 1.0;
+    }
     q.tol = e->tol;
     q.inner_tol = e->inner_tol;
     q.max_inner = e->max_inner;
@@ -692,6 +790,8 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
   }
   if (kind == OB2S_POISSON2D) {
     pois_init<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.b, n, q.pitch, seed);
+  } else if (kind == OB2S_HEAT2D) {  // u0 is the first right-hand side and first guess
+    heat_init<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.b, q.x, n, q.pitch, seed);
   } else {
     q.lambda = 1.0;
     q.steps = steps;
@@ -729,7 +829,7 @@ static int upload_work(ob2s_engine *e) {
   for (int k = 0; k < MAXA; k++) {
     if (!e->active[k]) continue;
     const Req &q = e->R[k];
-    if (q.kind == OB2S_POISSON2D) {
+    if (q.kind != OB2S_ADI3D) {
       w.pois_slot[w.npois] = k;
       w.pois_pref[w.npois + 1] = w.pois_pref[w.npois] + q.tiles;
       w.npois++;
@@ -756,7 +856,7 @@ OB2_API int ob2s_run(ob2s_engine *e, int iters, int *ids, int cap, int *n_done) 
   if (e->work_dirty && (err = upload_work(e))) return err;
   int variant = 0;
   for (int k = 0; k < MAXA; k++)
-    if (e->active[k]) variant |= e->R[k].kind == OB2S_POISSON2D ? 1 : 2;
+    if (e->active[k]) variant |= e->R[k].kind != OB2S_ADI3D ? 1 : 2;
   if (variant) {
     ob2s_engine::Graph *gr = nullptr;
     for (auto &g : e->graphs)
@@ -810,7 +910,7 @@ OB2_API int ob2s_fetch(ob2s_engine *e, int id, double *host, size_t count) {
   const Req &q = e->R[id];
   if (!q.done) return OB2S_ERR_NOTDONE;
   const int n = q.n;
-  if (q.kind == OB2S_POISSON2D) {
+  if (q.kind != OB2S_ADI3D) {
     if (count < (size_t)n * n) return OB2S_ERR_BADARG;
     double *tmp = nullptr;
     cudaError_t ce = cudaMallocAsync(&tmp, (size_t)n * n * 8, e->st);
@@ -839,7 +939,7 @@ OB2_API int ob2s_result_of(ob2s_engine *e, int id, ob2s_result *res) {
   res->outer = q.outer;
   res->rel_residual = q.rel;
   if (!q.done) return 0;
-  const size_t m = q.kind == OB2S_POISSON2D ? (size_t)q.n * q.n : (size_t)q.n * q.n * q.n;
+  const size_t m = q.kind != OB2S_ADI3D ? (size_t)q.n * q.n : (size_t)q.n * q.n * q.n;
   std::vector<double> h(m);
   int err = ob2s_fetch(e, id, h.data(), m);
   if (err) return err;

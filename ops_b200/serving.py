@@ -1,12 +1,14 @@
-"""Solve serving on one B200: continuous batching of Poisson / ADI requests.
+"""Solve serving on one B200: continuous batching of Poisson / heat / ADI requests.
 
     python -m ops_b200.serving [--requests 2000] [--rate R] [--mode mixed|fp64|both]
-                               [--budget-gb 160] [--iters 16] [--seed 6] [--json]
+                               [--budget-gb 160] [--iters 16] [--seed 6] [--heat-frac F]
 
 A request stream (seeded): Poisson-process arrivals; 70 % 2D Poisson solves
 (5-point, zero Dirichlet boundary, n log-uniform in [64, 2048], f ~ U(-1,1),
 relative residual 1e-8) and 30 % 3D ADI heat runs (n log-uniform in [32, 192],
-u0 ~ U(-1,1), 10 steps).  The serving loop keeps each admitted request's
+u0 ~ U(-1,1), 10 steps); --heat-frac F turns a share F of the requests into
+2D implicit heat runs (5 backward-Euler steps, each a CG solve to the same
+tolerance, sizes as Poisson).  The serving loop keeps each admitted request's
 arrays resident on the device and advances every active request in the same
 batched launches (libops_b200.so, ob2s_*).  Admission: a request joins as
 soon as it has arrived, a slot is free (OB2S_MAX_ACTIVE) and its bytes fit
@@ -36,7 +38,7 @@ from typing import Dict, List, Optional
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "libops_b200.so")
 
-POISSON2D, ADI3D = 0, 1
+POISSON2D, ADI3D, HEAT2D = 0, 1, 2
 FP64, MIXED = 0, 1
 MAX_ACTIVE = 128
 
@@ -159,34 +161,41 @@ class Request:
 
 
 def make_stream(count: int, rate: float, seed: int, adi_frac: float = 0.3,
-                pois_n=(64, 2048), adi_n=(32, 192), steps: int = 10) -> List[Request]:
+                pois_n=(64, 2048), adi_n=(32, 192), steps: int = 10,
+                heat_frac: float = 0.0, heat_steps: int = 5) -> List[Request]:
     """Seeded request stream: exponential inter-arrival times (rate per
-    second; rate <= 0: everything arrives at t = 0), kind by adi_frac, sizes
-    log-uniform over the ranges."""
+    second; rate <= 0: everything arrives at t = 0), kind by adi_frac (ADI)
+    and heat_frac (2D implicit heat, sizes as Poisson), the rest Poisson,
+    sizes log-uniform over the ranges.  With heat_frac = 0 the stream is
+    the same draw for draw as without the heat kind."""
     rng = random.Random(seed)
     t = 0.0
     out = []
     for k in range(count):
         if rate > 0:
             t += rng.expovariate(rate)
-        kind = ADI3D if rng.random() < adi_frac else POISSON2D
+        u = rng.random()
+        kind = ADI3D if u < adi_frac else (HEAT2D if u < adi_frac + heat_frac else POISSON2D)
         lo, hi = adi_n if kind == ADI3D else pois_n
         n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
-        out.append(Request(k, kind, n, 1000 + k, t, steps))
+        out.append(Request(k, kind, n, 1000 + k, t,
+                           heat_steps if kind == HEAT2D else steps))
     return out
 
 
 def request_bytes_moved(r: Request, mode: int) -> float:
-    """Algorithmic bytes of a finished request: CG iterations x bytes per
-    point per iteration (p' = r + beta p and w = A p' read r and p and write
-    p' and w; the update pass reads p' and w and updates x and r: FP64 80,
-    mixed 48 with FP32 r, w, p and the FP64 x) plus 24 B per point per FP64
-    residual pass; ADI 72 B per point per step (preproc reads u and writes du,
+    """Algorithmic bytes of a finished request.  Poisson / heat: per CG
+    iteration the single-reduction pass reads and writes r, w = A r, s = A p,
+    p and the iterate (mixed: FP32 vectors and the FP32 correction, 40 B per
+    point; FP64: 80 B); per residual replacement the FP64 residual pass reads
+    x, b and the correction and writes r, and the w = A r pass reads r and
+    writes w and folds the correction into x (mixed 24 + 32 B per point, FP64
+    24 + 16 B).  ADI: 72 B per point per step (preproc reads u and writes du,
     the x and y solves read and write du, the z solve reads du and updates
     u)."""
-    if r.kind == POISSON2D:
-        per = 48.0 if mode == MIXED else 80.0
-        return r.n * r.n * (per * r.iterations + 24.0 * (r.outer + 1))
+    if r.kind in (POISSON2D, HEAT2D):
+        per, outer = (40.0, 56.0) if mode == MIXED else (80.0, 40.0)
+        return r.n * r.n * (per * r.iterations + outer * (r.outer + 1))
     return r.n ** 3 * 72.0 * r.steps
 
 
@@ -229,7 +238,7 @@ def serve(engine: Engine, stream: List[Request], budget_bytes: int, iters: int =
             r.iterations, r.outer, r.rel, r.checksum = (res.iterations, res.outer,
                                                          res.rel_residual, res.checksum)
             if keep_solutions:
-                r.solution = engine.fetch(rid, r.n ** (2 if r.kind == POISSON2D else 3))
+                r.solution = engine.fetch(rid, r.n ** (3 if r.kind == ADI3D else 2))
             used -= engine.request_bytes(r.kind, r.n)
             engine.release(rid)
             done.append(r)
@@ -240,7 +249,7 @@ def serve(engine: Engine, stream: List[Request], budget_bytes: int, iters: int =
         return lat[min(len(lat) - 1, int(math.ceil(p / 100.0 * len(lat))) - 1)] if lat else 0.0
 
     moved = sum(request_bytes_moved(r, engine.mode) for r in done)
-    pois = [r for r in done if r.kind == POISSON2D]
+    pois = [r for r in done if r.kind in (POISSON2D, HEAT2D)]
     return {
         "requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
         "p50_s": pct(50), "p99_s": pct(99), "mean_s": sum(lat) / max(1, len(lat)),
@@ -270,14 +279,17 @@ def main(argv=None) -> int:
     ap.add_argument("--min-n", type=int, default=64, help="smallest Poisson grid")
     ap.add_argument("--max-n", type=int, default=2048, help="largest Poisson grid")
     ap.add_argument("--adi-frac", type=float, default=0.3, help="share of ADI requests")
+    ap.add_argument("--heat-frac", type=float, default=0.0,
+                    help="share of 2D implicit heat requests (5 backward-Euler steps each)")
     a = ap.parse_args(argv)
     stream_args = dict(count=a.requests, rate=a.rate, seed=a.seed, pois_n=(a.min_n, a.max_n),
-                       adi_frac=a.adi_frac)
+                       adi_frac=a.adi_frac, heat_frac=a.heat_frac)
     budget = int(a.budget_gb * 1e9)
     out = {"config": {"requests": a.requests, "rate": a.rate, "budget_gb": a.budget_gb,
                       "iters_per_replay": a.iters, "tile_y": a.tile_y,
                       "inner_tol": a.inner_tol, "seed": a.seed, "tol": 1e-8,
                       "poisson_n": [a.min_n, a.max_n], "adi_frac": a.adi_frac,
+                      "heat_frac": a.heat_frac,
                       "adi_n": [32, 192], "adi_steps": 10}}
     sols = {}
     if a.mode in ("mixed", "both"):

@@ -1,4 +1,4 @@
-"""CPU restatement of the serving engine's two request kinds (numpy).
+"""CPU restatement of the serving engine's three request kinds (numpy).
 
 TEST INFRASTRUCTURE ONLY: used by tests/ to check the engine
 (ops_b200/csrc/serve/ob2_serve.cu); nothing in the product imports it.
@@ -7,6 +7,10 @@ TEST INFRASTRUCTURE ONLY: used by tests/ to check the engine
     h = 1 / (n + 1), and the 5-point operator A x = 4 x - (neighbours) with a
     zero Dirichlet boundary; `relative_residual` measures ||b - A x|| / ||b||,
     the engine's stopping quantity, for a solution computed on the GPU.
+  * 2D implicit heat: u0 = 2 U - 1 from the hash (stream 3), each step solves
+    (1 + 4 rho) u' - rho (neighbours of u') = u with rho = dt / h^2 = 1 and a
+    zero Dirichlet boundary; `heat_steps` solves the same steps with a
+    direct sparse solver, `heat_relative_residual` measures one step.
   * 3D ADI heat step, after the reference's adi app: the right-hand side of
     apps/c/adi/preproc_kernel.h (d = lambda * (sum of the six neighbours -
     6 u) inside, 0 on the Dirichlet boundary; a = c = -lambda/2, b = 1 +
@@ -15,6 +19,12 @@ TEST INFRASTRUCTURE ONLY: used by tests/ to check the engine
     ops_tridMultiDimBatch / _Inc calls of apps/c/adi/adi.cpp:406-420).  The
     forward sweep multiplies by the precomputed 1/(b_i - a_i c'_{i-1}), as
     the engine does, so the arithmetic is the same operation for operation.
+    Deviation from the reference's adi app, stated: the serving engine's ADI
+    requests have constant coefficients, so it precomputes the Thomas
+    coefficients c'_i and 1 / (b_i - a_i c'_{i-1}) once per size and stores only
+    u and the right-hand side (72 B per point per step instead of the 216 B of
+    the adi app's per-point a, b, c arrays, which the ADI configuration of
+    apps/adi3d keeps); the solution is the same up to round-off.
 """
 
 from __future__ import annotations
@@ -102,3 +112,38 @@ def adi_steps(n: int, seed: int, steps: int, lam: float = 1.0) -> np.ndarray:
         d = thomas_along(d, 1, lam)  # y
         u = u + thomas_along(d, 0, lam)  # z, added to u
     return u
+
+
+HEAT_RHO = 1.0
+
+
+def heat_init(n: int, seed: int) -> np.ndarray:
+    """u0[j, i] of an n x n heat request."""
+    j, i = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    return 2.0 * hash_uniform(seed, i, j, 3) - 1.0
+
+
+def heat_apply(x: np.ndarray, rho: float = HEAT_RHO) -> np.ndarray:
+    p = np.zeros((x.shape[0] + 2, x.shape[1] + 2))
+    p[1:-1, 1:-1] = x
+    return (1.0 + 4.0 * rho) * p[1:-1, 1:-1] - rho * (p[1:-1, :-2] + p[1:-1, 2:] + p[:-2, 1:-1] +
+                                                      p[2:, 1:-1])
+
+
+def heat_relative_residual(x: np.ndarray, b: np.ndarray) -> float:
+    return float(np.linalg.norm(b - heat_apply(x)) / np.linalg.norm(b))
+
+
+def heat_steps(n: int, seed: int, steps: int, rho: float = HEAT_RHO) -> np.ndarray:
+    """the exact implicit steps (sparse direct solve) from heat_init"""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    e = np.ones(n)
+    t = sp.diags([-rho * e[:-1], -rho * e[:-1]], [-1, 1])
+    eye = sp.identity(n)
+    a = (sp.kron(eye, t) + sp.kron(t, eye) + (1.0 + 4.0 * rho) * sp.identity(n * n)).tocsc()
+    u = heat_init(n, seed).reshape(-1)
+    lu = spla.splu(a)
+    for _ in range(steps):
+        u = lu.solve(u)
+    return u.reshape(n, n)

@@ -7,6 +7,9 @@
   ||b - A x|| / ||b|| recomputed on the CPU (oracle/serving_oracle.py) from
   the fetched solution is at most 1e-8 (x 1.05 for the residual's own
   round-off), in FP64 and in the mixed form.
+* Heat requests (backward-Euler steps, each a CG solve): one step meets the
+  tolerance against u0 recomputed on the CPU, and several steps agree with
+  the same steps solved by a sparse direct solver to the solve accuracy.
 * ADI requests match the CPU restatement of the reference's adi step
   (preproc + x/y/z Thomas, z added to u) to 1e-13 of the field's scale
   (same operations in the same order, IEEE without contraction).
@@ -43,6 +46,7 @@ def test_result_same_alone_and_in_mix(mode):
         # the same request among others; more join while it runs
         others = [eng.submit(serving.POISSON2D, n, 20 + n) for n in (64, 333, 97)]
         others.append(eng.submit(serving.ADI3D, 40, 7, 4))
+        others.append(eng.submit(serving.HEAT2D, 90, 8, 2))
         b = eng.submit(serving.POISSON2D, 150, 11)
         eng.run(5)
         others += [eng.submit(serving.POISSON2D, 211, 5), eng.submit(serving.ADI3D, 33, 9, 3)]
@@ -87,6 +91,31 @@ def test_mixed_matches_fp64_solution():
     d = np.max(np.abs(sol[serving.MIXED] - sol[serving.FP64])) / np.max(np.abs(sol[serving.FP64]))
     # both meet 1e-8 in the residual; the solutions agree to the solve accuracy
     assert d < 1e-6, d
+
+
+@pytest.mark.parametrize("mode", [serving.FP64, serving.MIXED])
+def test_heat_requests(mode):
+    eng = serving.Engine(mode)
+    try:
+        one = eng.submit(serving.HEAT2D, 190, 31, 1)
+        three = eng.submit(serving.HEAT2D, 77, 32, 3)
+        pois = eng.submit(serving.POISSON2D, 120, 33)
+        res = finish_all(eng)
+        x = eng.fetch(one, 190 * 190).reshape(190, 190)
+        rel = so.heat_relative_residual(x, so.heat_init(190, 31))
+        assert rel <= 1.05e-8, (rel, res[one].rel_residual)
+        # A >= I, so each step's error is at most its residual (1e-8 of its
+        # right-hand side, whose norm never grows): three steps add up to
+        # 3e-8 of ||u0|| at most
+        u = eng.fetch(three, 77 * 77).reshape(77, 77)
+        ref = so.heat_steps(77, 32, 3)
+        assert np.linalg.norm(u - ref) <= 3 * 1.05e-8 * np.linalg.norm(so.heat_init(77, 32))
+        xp = eng.fetch(pois, 120 * 120).reshape(120, 120)
+        assert so.relative_residual(xp, 33) <= 1.05e-8
+        for rid in (one, three, pois):
+            eng.release(rid)
+    finally:
+        eng.close()
 
 
 @pytest.mark.parametrize("n,steps", [(24, 3), (41, 2), (70, 1)])
