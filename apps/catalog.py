@@ -6,6 +6,9 @@ Flavours
   oracle   the CPU oracle: oracle/include/ops_seq_v2.h + liboracle_ops.so
   ref_seq  the reference's own sequential backend (ops_seq_v2.h + libops_seq.a)
   ref_omp  the reference's own OpenMP backend (legacy translator + libops_seq.a)
+  ref_cuda the reference's own CUDA backend (legacy translator's CUDA kernels +
+           libops_cuda.a, sm_100): a same-machine measure of the reference's GPU
+           code, reported as context
 
 Applications are either this repository's drivers under apps/ (our code, on the
 unchanged OPS API) or reference applications, whose sources are read from the
@@ -75,6 +78,16 @@ APPS = {
     "ref_adi_burger3d": ("ref", os.path.join(_REF_ROOT, "apps", "c", "adi_burger_3D"),
                          ["adi_burger_3D.cpp"], None),
     "ref_tti": ("ref", os.path.join(_REF_ROOT, "apps", "c", "tti"), ["tti.cpp"], None),
+    # half-precision dats (ACC<half>): Jacobi on a 4094^2 grid in binary16
+    "ref_halfprecision": ("ref", os.path.join(_REF_ROOT, "apps", "c", "halfprecision"),
+                          ["laplace2d.cpp"], None),
+    # multi-block shsgc (halo transfers between the blocks every step)
+    "ref_mb_shsgc": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mb_shsgc", "Max_datatransfer"),
+                     ["shsgc.cpp"], None),
+    # the lattice-Boltzmann tutorial app (final step), the OpenSBLI wave test
+    "ref_lbm": ("ref", os.path.join(_REF_ROOT, "apps", "c", "ops-lbm", "step5"),
+                ["lattboltz2d.cpp"], None),
+    "ref_wave": ("ref", os.path.join(_REF_ROOT, "apps", "c", "wave_test"), ["opensbli.cpp"], None),
     # reference applications written with the original OPS_ACCn kernel API
     # (b200 flavour only: the oracle restates the ACC<> API)
     "ref_tealeaf": ("ref", os.path.join(_REF_ROOT, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
@@ -146,6 +159,26 @@ def ensure_ref_lib() -> str:
     return os.path.join(REF_OUT, "lib", "libops_seq.a")
 
 
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+# the reference's default CUDA flags (makefiles/Makefile.cuda:15-18) for sm_100
+REF_NVCCFLAGS = ["-Xcompiler=-fPIC", "-O3", "-g", "-std=c++14",
+                 "-gencode", "arch=compute_100,code=sm_100", "-w"]
+
+
+def ensure_ref_cuda_lib() -> str:
+    """The reference's own CUDA backend (libops_cuda.a, oracle/ref/Makefile
+    cudalib): a same-machine measure of the reference's GPU code."""
+    lib = os.path.join(REF_OUT, "lib", "libops_cuda.a")
+    if not REF or not os.path.isdir(REF):
+        if os.path.exists(lib):
+            return lib
+        raise RuntimeError("reference tree not present (set OPS_REFERENCE_TREE)")
+    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "cudalib", "-j8",
+          "REF=" + REF])
+    return lib
+
+
 def _deps(name: str, flavour: str):
     d, paths = sources_of(name)
     deps = list(paths)
@@ -214,8 +247,10 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
             link[1:1] = ["-shared", "-Wl,-Bsymbolic"]
         _run(link)
         return target
-    if flavour in ("ref_seq", "ref_omp"):
+    if flavour in ("ref_seq", "ref_omp", "ref_cuda"):
         lib = ensure_ref_lib()
+        if flavour == "ref_cuda":
+            lib = ensure_ref_cuda_lib()
         rinc = os.path.join(REF, "ops", "c", "include")
         srcdir = os.path.join(out, "src")
         if os.path.isdir(srcdir):
@@ -228,13 +263,21 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
                     if p != CLOVER_STEP_SRC]
         flags = ["-O3", "-std=c++14", "-fPIC", "-w", "-fopenmp", "-Dgnu", "-I" + rinc, "-I" + srcdir,
                  "-I" + APPS_DIR]
-        if flavour == "ref_omp":
+        pre_objs = []
+        if flavour in ("ref_omp", "ref_cuda"):
             trans = APPS[name][3] or APPS[name][2]
             _run([sys.executable, os.path.join(REF, "ops_translator_legacy", "c", "ops.py"),
                   *trans], cwd=srcdir)
             objs_src = [os.path.join(srcdir, (s[:-4] + "_ops.cpp") if s in trans else s)
                         for s in APPS[name][2]]
-            objs_src.append(os.path.join(srcdir, "mpi_openmp", "mpi_openmp_kernels.cpp"))
+            if flavour == "ref_omp":
+                objs_src.append(os.path.join(srcdir, "mpi_openmp", "mpi_openmp_kernels.cpp"))
+            else:  # the legacy translator's CUDA kernels (Makefile.c_app_legacy:282-283)
+                ko = os.path.join(out, "cuda_kernels_cu.o")
+                _run([NVCC, *REF_NVCCFLAGS, "-I" + rinc, "-I" + srcdir, "-c", "-o", ko,
+                      os.path.join(srcdir, "cuda", "cuda_kernels.cu")])
+                pre_objs.append(ko)
+                flags += ["-I" + os.path.join(CUDA_HOME, "include")]
         if name == "clover_step":
             objs_src.append(CLOVER_STEP_SRC)
         objs = []
@@ -245,9 +288,14 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
                 cmd += extra_defs
             if name == "clover_step" and p == CLOVER_STEP_SRC:
                 cmd += ["-DCLOVER_STEP_REFERENCE"]
+                if flavour == "ref_cuda":
+                    cmd += ["-DCLOVER_STEP_CUDA", "-I" + os.path.join(CUDA_HOME, "include")]
             _run(cmd + ["-c", p, "-o", o])
             objs.append(o)
-        link = ["g++", "-fopenmp", "-o", target, *objs, lib]
+        link = ["g++", "-fopenmp", "-o", target, *pre_objs, *objs, lib]
+        if flavour == "ref_cuda":
+            link += ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart", "-lcurand",
+                     "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")]
         if shared:
             link[1:1] = ["-shared", "-Wl,-Bsymbolic"]
         _run(link)

@@ -1,6 +1,6 @@
 """Run the CloverLeaf step harness (apps/clover_step) in one flavour.
 
-    python -m apps.clover_run --flavour b200|oracle|ref_omp --cells N --steps K
+    python -m apps.clover_run --flavour b200|oracle|ref_omp|ref_cuda --cells N --steps K
                               [--warmup W] [--seed S] [--dump FILE] [--fetch-dump FILE]
                               [--threads T]
 
@@ -101,8 +101,10 @@ def main(argv=None):
     L.clover_step_setup(1, argv_c)
     if a.warmup:
         L.clover_step_run(a.warmup)
+    L.clover_step_sync()
     t0 = time.perf_counter()
     L.clover_step_run(a.steps)
+    L.clover_step_sync()
     t1 = time.perf_counter()
     L.clover_step_summary()
     if a.fetch_dump:

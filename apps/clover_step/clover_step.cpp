@@ -17,6 +17,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <unistd.h>
+#if defined(CLOVER_STEP_CUDA)
+#include <cuda_runtime_api.h>
+#endif
 
 #define OPS_2D
 #include "ops_seq_v2.h"
@@ -86,6 +89,18 @@ __attribute__((visibility("default"))) void clover_step_summary(void) {
   complete = TRUE;
   field_summary();
   fflush(g_out);
+}
+
+/* Waits until every step issued so far has finished on the device (the
+ * reference's CUDA backend returns from a loop before its kernel ends;
+ * this backend's ops_timers flushes its queue and waits for the device). */
+__attribute__((visibility("default"))) void clover_step_sync(void) {
+#if defined(CLOVER_STEP_CUDA)
+  cudaDeviceSynchronize();
+#else
+  double c, e;
+  ops_timers(&c, &e);
+#endif
 }
 
 __attribute__((visibility("default"))) int clover_step_current(void) { return step; }

@@ -18,6 +18,9 @@ par_loops, all host cores) for poisson_2x2 (full config) and cg_heat_4096
 CPU restatement of the Thomas solves for adi_256 (the reference's
 tridiagonal solver is an external library absent from its tree), one step.
 The serving configuration's baseline is its own FP64 one-at-a-time run.
+
+  reference_cuda_cloverleaf   the headline CloverLeaf configuration on the
+                reference's own CUDA backend on the same GPU (context only)
 """
 
 from __future__ import annotations
@@ -192,8 +195,28 @@ def serving(clock, peak, cores, baseline=True, requests=2000, rate_requests=600)
     return e
 
 
+def reference_cuda_cloverleaf(clock, peak, cores, baseline=True, cells=3840, steps=20,
+                              warmup=5):
+    """Context, not a baseline of the record: the headline CloverLeaf
+    configuration on the reference's own CUDA backend (its legacy
+    translator's CUDA kernels and libops_cuda, built from the reference
+    sources for sm_100 with its default flags), on this GPU, host wall clock
+    around the steps with a device synchronisation at both ends."""
+    clock.start()
+    out, _ = _run([sys.executable, "-m", "apps.clover_run", "--flavour", "ref_cuda", "--cells",
+                   str(cells), "--steps", str(steps), "--warmup", str(warmup)])
+    clk = clock.stop()
+    r = json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+    ms = r["s_per_step"] * 1e3
+    return {"metric": "GLUPS", "value": cells * cells / (ms * 1e-3) / 1e9, "unit": "GLUPS",
+            "ms_per_step": ms, "clocks": clk, "summary": r["summary"],
+            "workload": "cloverleaf2d_hydro %dx%d, %d steps after %d warm-up steps, the "
+                        "reference's CUDA backend on this GPU (context for the headline line)"
+                        % (cells, cells, steps, warmup)}
+
+
 CONFIGS = {"poisson_2x2": poisson_2x2, "adi_256": adi_256, "cg_heat_4096": cg_heat_4096,
-           "serving": serving}
+           "serving": serving, "reference_cuda_cloverleaf": reference_cuda_cloverleaf}
 
 
 def run_all(names, clock, peak, cores, baseline=True):

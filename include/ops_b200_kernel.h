@@ -20,6 +20,7 @@
 #include <limits.h>
 
 #include "ops_lib_core.h"
+#include "ops_b200_loop.h"
 
 namespace ob2 {
 
@@ -123,6 +124,90 @@ __device__ __forceinline__ void final_combine(int dim, const T *part, T *acc, in
 __device__ __forceinline__ void reset_counter(unsigned int *counter) {
   const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   if (t == 0) *counter = 0u;
+}
+
+/* ---- halo group folded into a loop launch (ob2_hfuse, ops_b200_loop.h) ----
+ * Copies the cells of the folded group that lie in this CTA's footprint: the
+ * CTA's tile [x0,x1) x [y0,y1) x [z0,z1) in loop coordinates widened by the
+ * loop's stencil reach.  A cell is located exactly as the halo transfer
+ * kernel locates it (destination storage index start + t or, flipped,
+ * start + L - 1 - t along each dimension); overlapping footprints copy the
+ * same value from the same source.  The caller synchronises the CTA before
+ * the loop reads the copied cells. */
+__device__ __forceinline__ void hfuse_copy(const ob2_halo_task &T, const long long *s,
+                                           const int *t) {
+  long long so = 0, dof = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const int a = T.src_axis[i];
+    const int ti = T.src_flip[i] ? T.iter[a] - 1 - t[a] : t[a];
+    so += (long long)(T.src_start[i] + ti) * T.src_cum[i];
+    dof += s[i] * T.dst_cum[i];
+  }
+  for (int c = 0; c < T.ncomp; c++) {
+    const long long se = T.src_soa ? so + c * T.src_npts_total : so * T.ncomp + c;
+    const long long de = T.dst_soa ? dof + c * T.dst_npts_total : dof * T.ncomp + c;
+    const char *sp = T.src + se * T.src_type;
+    char *dp = T.dst + de * T.dst_type;
+    if (T.src_type == T.dst_type) {
+      if (T.src_type == 8)
+        *(unsigned long long *)dp = *(const unsigned long long *)sp;
+      else if (T.src_type == 4)
+        *(unsigned int *)dp = *(const unsigned int *)sp;
+      else if (T.src_type == 2)
+        *(unsigned short *)dp = *(const unsigned short *)sp;
+      else
+        for (int b = 0; b < T.src_type; b++) dp[b] = sp[b];
+    } else {
+      const double v = T.src_type == 8   ? *(const double *)sp
+                       : T.src_type == 2 ? (double)__half2float(*(const __half *)sp)
+                                         : (double)*(const float *)sp;
+      if (T.dst_type == 8)
+        *(double *)dp = v;
+      else if (T.dst_type == 2)
+        *(__half *)dp = __double2half(v);
+      else
+        *(float *)dp = (float)v;
+    }
+  }
+}
+
+__device__ __forceinline__ void hfuse_prologue(const ob2_hfuse &h, int inst, int x0, int x1,
+                                               int y0, int y1, int z0, int z1) {
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;  // no points: no footprint
+  const int flo[3] = {x0 - h.mlo[0], y0 - h.mlo[1], z0 - h.mlo[2]};
+  const int fhi[3] = {x1 + h.mhi[0], y1 + h.mhi[1], z1 + h.mhi[2]};
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  for (int e = 0; e < h.n; e++) {
+    if (h.inst[e] != inst) continue;
+    const ob2_halo_task &T = h.tasks[h.task[e]];
+    int lo[3], cnt[3];
+    long long total = 1;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {  // the task's cells along dim i, in loop coordinates
+      const int a = h.org[e][i] + T.dst_start[i];
+      const int b = a + T.iter[T.dst_axis[i]];
+      lo[i] = max(a, flo[i]);
+      cnt[i] = max(0, min(b, fhi[i]) - lo[i]);
+      total *= cnt[i];
+    }
+    for (long long k = tid; k < total; k += nt) {
+      long long s[3];
+      int t[3];
+      long long rem = k;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int off = (int)(rem % cnt[i]);
+        rem /= cnt[i];
+        s[i] = (long long)(lo[i] + off - h.org[e][i]);  // destination storage index
+        const int ti = (int)(s[i] - T.dst_start[i]);
+        const int a = T.dst_axis[i];
+        t[a] = T.dst_flip[i] ? T.iter[a] - 1 - ti : ti;
+      }
+      hfuse_copy(T, s, t);
+    }
+  }
 }
 
 }  // namespace ob2

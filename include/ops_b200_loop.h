@@ -46,6 +46,30 @@ typedef int (*ob2_flauncher)(int n, const int *ids, const void *const *params,
                              const size_t *psize, const unsigned *grids, const unsigned *block,
                              int idx32, void *stream);
 
+/* A halo group folded into the launch of the loop that consumes it (the
+ * multi-block case: ops_halo_transfer followed by a loop over the blocks
+ * that reads the halos just filled).  Each CTA first copies the group's
+ * cells that fall in its own footprint (its tile widened by the loop's
+ * stencil reach), then runs the loop; the runtime folds a group only when
+ * every cell of it lies in some footprint and the loop writes no dat the
+ * group reads or fills, so the result equals running the transfer first.
+ * Entry e: task task[e] of the group's device task table, whose destination
+ * is read by instance inst[e] of the launch; org[e] is the loop coordinate
+ * of the destination dat's storage index 0 along each axis. */
+#define OB2_HFUSE_MAX 32
+typedef struct ob2_hfuse {
+  const ob2_halo_task *tasks;
+  int n;
+  int task[OB2_HFUSE_MAX];
+  int inst[OB2_HFUSE_MAX];
+  int org[OB2_HFUSE_MAX][3];
+  int mlo[3], mhi[3];  /* stencil reach below / above along each axis (>= 0) */
+} ob2_hfuse;
+/* A generated halo-folding launcher: as ob2_mlauncher, with the folded
+ * group h. */
+typedef int (*ob2_hlauncher)(const void *const *params, int n, const unsigned *grid,
+                             const unsigned *block, const ob2_hfuse *h, void *stream);
+
 typedef struct ob2_loop {
   const char *name;
   int kernel_index;  /* timing-table slot */
@@ -78,6 +102,8 @@ typedef struct ob2_loop {
   int fuse_id;              /* the loop's id in the fused launcher, -1: none */
   ob2_flauncher ffn;        /* the application's fused launcher (set by the
                                stub before ob2_launch; NULL: none) */
+  ob2_hlauncher hfn;        /* the loop's halo-folding launcher (set by the
+                               stub before ob2_launch; NULL: none) */
 } ob2_loop;
 
 /* A generated launcher: launches one kernel variant with the parameter block
@@ -109,7 +135,10 @@ typedef int (*ob2_mlauncher)(const void *const *params, int n, const unsigned *g
  * that share no point of a dat that one of them writes -- each loop writes
  * its range and reads its range shifted by every stencil point -- run as one
  * launch of the application's fused launcher L->ffn (OPS_B200_FUSE=0: off);
- * the boundary loops of a halo update are the typical case.
+ * the boundary loops of a halo update are the typical case.  A queued halo
+ * transfer followed by a run of instances whose loop reads the halos it
+ * fills is folded into that run's launch (L->hfn, ob2_hfuse;
+ * OPS_B200_HFUSE=0: off).
  * rows_per_thread: points each thread covers along y (the grid's y extent
  * is derived from it per tile). */
 OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const void *params,

@@ -9,9 +9,10 @@
  *                   ||h^2 f - A u|| / ||h^2 f|| <= tol;
  *   OB2S_HEAT2D     `steps` backward-Euler steps of the 2D heat equation on
  *                   an n x n grid with dt = h^2: each step solves
- *                   (1 + 4) u' - (sum of the 4 neighbours of u') = u by
- *                   conjugate gradients to the same tolerance, from
- *                   u0 ~ U(-1,1) (the seed) and a zero Dirichlet boundary;
+ *                   5 u' - (sum of the 4 neighbours of u') = u by conjugate
+ *                   gradients to `tol` relative to that step's right-hand
+ *                   side, from u0 ~ U(-1,1) (the seed), zero Dirichlet
+ *                   boundary;
  *   OB2S_ADI3D      `steps` steps of the 3D ADI heat scheme on an n^3 grid
  *                   (the reference's adi app: preproc_kernel.h, then
  *                   tridiagonal solves along x, y and z with the z solution
@@ -27,18 +28,15 @@
  * batching: new requests join at the next ob2s_run, finished ones stop
  * consuming work immediately).
  *
- * Conjugate gradients run in the single-reduction form of Chronopoulos and
- * Gear (one pass over the vectors and one scalar step per iteration).
- * Precision modes (FP64 iterate x):
- *   OB2S_FP64   CG vectors in FP64, x updated every iteration (the plain form);
- *   OB2S_MIXED  CG vectors r, w = A r, s = A p, p stored in FP32 (each value
- *               formed in FP64 and rounded once; dot products accumulated
- *               in FP64); alpha p accumulates in an FP32 correction that is
- *               folded into the FP64 x whenever the recursive residual has
- *               dropped by `inner_tol` since the last true residual (or meets
- *               `tol`); the residual is then replaced by b - A x computed in
- *               FP64 (iterative refinement that keeps the search
- *               directions), and convergence is tested on that residual.
+ * Precision modes (conjugate gradients, FP64 iterate x):
+ *   OB2S_FP64   CG in FP64 (the plain form);
+ *   OB2S_MIXED  FP32 CG vectors r, w, p and their arithmetic (dot
+ *               products accumulated in FP64), FP64 iterate x updated in
+ *               FP64; whenever the recursive residual has dropped by
+ *               `inner_tol` since the last true residual (or meets `tol`),
+ *               the residual is replaced by b - A x computed in FP64
+ *               (iterative refinement that keeps the Krylov directions);
+ *               convergence is tested on that FP64 residual.
  * Both modes use the same replacement schedule; `max_inner` caps the CG
  * iterations of a request.
  * ADI requests run in FP64 in both modes (constant coefficients: only u and
@@ -70,7 +68,7 @@ typedef struct ob2s_engine ob2s_engine;
 
 typedef struct ob2s_result {
   int kind, n, done;
-  int iterations;      /* CG iterations (over all time steps for heat) / ADI steps */
+  int iterations;      /* CG iterations (all time steps of a heat request) / ADI steps */
   int outer;           /* residual evaluations in FP64 (refinement passes) */
   double rel_residual; /* final FP64 relative residual (Poisson) */
   double checksum;     /* sum of the interior solution */

@@ -54,6 +54,21 @@
 #endif
 #endif
 
+/* The 16-bit `half` element type of half-precision dats (the choice of
+ * ops_lib_core.h:96-118 of the reference): CUDA's __half in code nvcc
+ * compiles (kernels and their stubs), the compiler's IEEE binary16
+ * _Float16 in host code, so that both sides share the 2-byte layout. */
+#if defined(__CUDACC__)
+#ifndef __HALF_DEFINED__
+#include <cuda_fp16.h>
+#endif
+typedef __half half;
+#elif defined(__STDCPP_FLOAT16_T__) || defined(FLT16_MIN) || defined(__FLT16_MIN__)
+typedef _Float16 half;
+#else
+typedef uint16_t half;
+#endif
+
 #ifdef __cplusplus
 #define OPS_EXTERN_C extern "C"
 #else
@@ -446,6 +461,7 @@ inline int type_error(const ull *, const char *t) {
   return !(strcmp(t, "ull") == 0 || strcmp(t, "unsigned long long") == 0);
 }
 inline int type_error(const bool *, const char *t) { return strcmp(t, "bool"); }
+inline int type_error(const half *, const char *t) { return strcmp(t, "half"); }
 
 /* ops_lib_core.h:648-694 */
 template <class T>

@@ -2,6 +2,7 @@
 // device selection, the work stream, memory, events, halo transfer, box
 // copies and fills.  Kernels here are HBM-bound byte/element moves: no tensor
 // cores; coalesced along x, grids sized from the SM count.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -123,6 +124,7 @@ __device__ __forceinline__ long long storage_offset(const int *axis, const int *
 
 __device__ __forceinline__ double load_as_double(const char *p, int ts) {
   if (ts == 8) return *(const double *)p;
+  if (ts == 2) return (double)__half2float(*(const __half *)p);
   return (double)*(const float *)p;
 }
 
@@ -156,6 +158,8 @@ __global__ void halo_kernel(const ob2_halo_task *__restrict__ tasks) {
         double v = load_as_double(sp, T.src_type);
         if (T.dst_type == 8)
           *(double *)dp = v;
+        else if (T.dst_type == 2)
+          *(__half *)dp = __double2half(v);
         else
           *(float *)dp = (float)v;
       }

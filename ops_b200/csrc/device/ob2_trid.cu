@@ -670,16 +670,24 @@ int launch_pipe(const Lines &g, const void *a, const void *b, const void *c, voi
   return (int)cudaGetLastError();
 }
 
-// OB2_TRID_PIPE: 1 (default) solves lines of 2 to 256 points with the
-// pipelined persistent kernel, for strided and unit-stride lines and both
-// element sizes; 0 keeps the kernels below.
+// OB2_TRID_PIPE: 1 (default) solves strided lines of 2 to 256 points with
+// the pipelined persistent kernel, 2 unit-stride lines too, 0 neither.
+// Measured on the 256^3 ADI solves (CUDA events, FP64): y 244 / z 372 us
+// against 258 / 381 us for the line-major CTA kernel, and the FP32-storage
+// step 1.117 against 1.166 ms; unit-stride x lines 451 us against 318 us for
+// the warp-per-line kernel (the chunk-per-lane copies are 8-byte elements
+// 64 bytes apart), so x stays on the latter.  ncu (ADI 256^3, y solve): 24 %
+// of the warp slots active (108-118 registers, 108 KB of shared memory: two
+// CTAs per SM), the stalls split between shared-memory and CTA barriers of
+// the PCR and the FP64 divisions: latency-bound, not memory-bound.
 bool use_pipe(const Lines &g) {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("OB2_TRID_PIPE");
     v = e ? atoi(e) : 1;
   }
-  return v == 1 && g.n >= 2 && g.n <= 32 * kPipeCL;
+  if (g.n < 2 || g.n > 32 * kPipeCL) return false;
+  return g.unit ? v == 2 : v >= 1;
 }
 
 // OB2_TRID_STRIDED: how strided lines are solved.  Measured on the 256^3

@@ -70,6 +70,11 @@ struct GroupX {
   int ntasks = 0;
   long long max_pts = 0;
   std::vector<char *> key;  // dat device pointers the table was built for
+  // per task, for folding the group into a consuming loop launch: source
+  // and destination dat, the destination's loop coordinate of storage index
+  // 0 and its box in loop coordinates
+  std::vector<int> src_dat, dst_dat;
+  std::vector<std::array<int, 3>> org, dlo, dhi;
 };
 
 struct Runtime {
@@ -136,6 +141,8 @@ struct Runtime {
     int lo[3], hi[3];
     std::vector<QAcc> acc;
     void *tasks; int ntasks; long long max_pts;  // halo group
+    int group;              // halo group index
+    ob2_hlauncher hfn;      // halo-folding launcher (NULL: none)
   };
   std::vector<QItem> q;
   struct Graph {
@@ -149,6 +156,8 @@ struct Runtime {
   bool fuse = true;           // run independent small loops in one launch
   long long fuse_pts = 65536; // largest loop (points) that is fused
   long long fused_launches = 0, fused_loops = 0;
+  bool hfuse = true;          // fold halo transfers into the consuming launch
+  long long hfused = 0;       // halo transfers folded
 };
 
 Runtime *R = nullptr;
@@ -595,10 +604,97 @@ void run_fused(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
   r.fused_loops += n;
 }
 
+// Folding the halo group q[h] into the launch of loop items [b, e) (one
+// loop, its instances on several blocks): legal when every task's
+// destination dat is read (OPS_READ) by one of the instances, every cell the
+// task fills lies inside that instance's range widened by the loop's stencil
+// reach (so some CTA's footprint holds it), and no instance writes a dat the
+// group reads or fills.  Fills h and returns true when legal.
+bool hfuse_plan(const std::vector<Runtime::QItem> &q, size_t hi, size_t b, size_t e,
+                ob2_hfuse &h) {
+  Runtime &r = rt();
+  const Runtime::QItem &H = q[hi];
+  if (!r.hfuse || H.kind != 1 || H.group < 0 || b >= e) return false;
+  const GroupX &gx = r.groupx[H.group];
+  if (gx.ntasks <= 0 || gx.ntasks > OB2_HFUSE_MAX || (int)gx.dst_dat.size() != gx.ntasks)
+    return false;
+  for (size_t k = b; k < e; k++)
+    if (q[k].kind != 0 || !q[k].hfn || q[k].hfn != q[b].hfn) return false;
+  memset(&h, 0, sizeof(h));
+  // stencil reach of every read argument, per axis
+  for (size_t k = b; k < e; k++)
+    for (auto &a : q[k].acc) {
+      if (a.any || a.flat || a.mg) return false;
+      if (a.acc != OPS_READ) {
+        for (int t = 0; t < gx.ntasks; t++)
+          if (a.dat == gx.src_dat[t] || a.dat == gx.dst_dat[t]) return false;
+        continue;
+      }
+      if (a.sidx < 0) continue;
+      const ops_stencil_core *st = r.stencils[a.sidx];
+      for (int p = 0; p < st->points; p++)
+        for (int d = 0; d < st->dims && d < 3; d++) {
+          const int o = st->stencil[p * st->dims + d];
+          h.mlo[d] = std::max(h.mlo[d], -o);
+          h.mhi[d] = std::max(h.mhi[d], o);
+        }
+    }
+  h.tasks = (const ob2_halo_task *)H.tasks;
+  h.n = gx.ntasks;
+  for (int t = 0; t < gx.ntasks; t++) {
+    int inst = -1;
+    for (size_t k = b; k < e && inst < 0; k++)
+      for (auto &a : q[k].acc)
+        if (a.dat == gx.dst_dat[t] && a.acc == OPS_READ) {
+          inst = (int)(k - b);
+          break;
+        }
+    if (inst < 0) return false;
+    const Runtime::QItem &L = q[b + inst];
+    for (int d = 0; d < 3; d++) {
+      const int lo = d < L.ndim ? L.lo[d] - h.mlo[d] : 0;
+      const int hi = d < L.ndim ? L.hi[d] + h.mhi[d] : 1;
+      if (gx.dlo[t][d] < lo || gx.dhi[t][d] > hi) return false;
+      h.org[t][d] = gx.org[t][d];
+    }
+    h.task[t] = t;
+    h.inst[t] = inst;
+  }
+  for (int d = 0; d < 3; d++)
+    if (d >= q[b].ndim) h.mlo[d] = h.mhi[d] = 0;
+  return true;
+}
+
+void run_hfused(std::vector<Runtime::QItem> &q, size_t b, size_t e, const ob2_hfuse &h) {
+  Runtime &r = rt();
+  const void *prm[OB2_MULTI_MAX];
+  unsigned g[3] = {0, 0, 0};
+  for (size_t k = b; k < e; k++) {
+    prm[k - b] = q[k].prm.data();
+    for (int d = 0; d < 3; d++) g[d] = std::max(g[d], q[k].grid[d]);
+  }
+  void *ev = r.capturing ? nullptr : kt_begin();
+  check(q[b].hfn(prm, (int)(e - b), g, q[b].block, &h, ob2_dev_stream()),
+        "ops_par_loop launch (with halo transfer)");
+  r.launches++;
+  r.hfused++;
+  if (e - b > 1) r.multi_launches++;
+  kt_end(ev, q[b].kidx);
+}
+
 void run_queue(std::vector<Runtime::QItem> &q) {
   Runtime &r = rt();
   size_t i = 0;
   while (i < q.size()) {
+    if (q[i].kind == 1 && i + 1 < q.size() && q[i + 1].kind == 0 && !r.tiling) {
+      const size_t j = multi_run(q, i + 1);
+      ob2_hfuse h;
+      if (hfuse_plan(q, i, i + 1, j, h)) {
+        run_hfused(q, i + 1, j, h);
+        i = j;
+        continue;
+      }
+    }
     if (r.tiling && tileable(q[i])) {
       size_t j = i + 1;
       while (j < q.size() && tileable(q[j]) && q[j].ndim == q[i].ndim) j++;
@@ -658,6 +754,8 @@ OPS_API void ob2_flush(void) {
     put(&it.mfn, sizeof it.mfn);
     put(&it.ffn, sizeof it.ffn);
     put(&it.fid, sizeof it.fid);
+    put(&it.hfn, sizeof it.hfn);
+    put(&it.group, sizeof it.group);
     const size_t np = it.prm.size();
     put(&np, sizeof np);
     put(it.grid, sizeof it.grid);
@@ -763,6 +861,8 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
   it.tasks = nullptr;
   it.ntasks = 0;
   it.max_pts = 0;
+  it.group = -1;
+  it.hfn = L->hfn;
   const int td = L->dim - 1;
   for (int i = 0; i < L->nargs; i++) {
     ops_arg &a = L->args[i];
@@ -848,6 +948,7 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_AUTOTUNE"))) r.autotune = atoi(e) != 0;
   if ((e = getenv("OPS_B200_MULTI"))) r.multi = atoi(e) != 0;
   if ((e = getenv("OPS_B200_FUSE"))) r.fuse = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_HFUSE"))) r.hfuse = atoi(e) != 0;
   if ((e = getenv("OPS_B200_FUSE_PTS"))) r.fuse_pts = atoll(e);
   if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
     r.tune_file = e;
@@ -1233,6 +1334,11 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
   std::vector<ob2_halo_task> tasks;
   gx.key.clear();
   gx.max_pts = 0;
+  gx.src_dat.clear();
+  gx.dst_dat.clear();
+  gx.org.clear();
+  gx.dlo.clear();
+  gx.dhi.clear();
   for (int hh = 0; hh < g->nhalos; hh++) {
     ops_halo h = g->halos[hh];
     for (int i = 3; i < OPS_MAX_DIM; i++)
@@ -1248,8 +1354,13 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
     t.src_type = h->from->type_size;
     t.dst_type = h->to->type_size;
     if (t.src_type != t.dst_type) {
-      bool okf = (!strcmp(h->from->type, "double") || !strcmp(h->from->type, "float")) &&
-                 (!strcmp(h->to->type, "double") || !strcmp(h->to->type, "float"));
+      // mixed float / double / half transfers convert each value to the
+      // destination type (ops_host_singlenode.cpp:224-228, through the
+      // smaller of the two types, which equals the direct conversion)
+      auto fp = [](const char *t) {
+        return !strcmp(t, "double") || !strcmp(t, "float") || !strcmp(t, "half");
+      };
+      bool okf = fp(h->from->type) && fp(h->to->type);
       if (!okf)
         throw OPSException(OPS_NOT_IMPLEMENTED, "Error: unsupported mixed-type halo transfer");
       t.float_kind = 1;
@@ -1290,6 +1401,19 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
       }
     }
     if (t.npts > gx.max_pts) gx.max_pts = t.npts;
+    {
+      std::array<int, 3> og, lo, hi;
+      for (int i = 0; i < 3; i++) {
+        og[i] = h->to->d_m[i] + h->to->base[i];
+        lo[i] = og[i] + t.dst_start[i];
+        hi[i] = lo[i] + t.iter[t.dst_axis[i]];
+      }
+      gx.org.push_back(og);
+      gx.dlo.push_back(lo);
+      gx.dhi.push_back(hi);
+      gx.src_dat.push_back(h->from->index);
+      gx.dst_dat.push_back(h->to->index);
+    }
     tasks.push_back(t);
     gx.key.push_back(h->from->data_d);
     gx.key.push_back(h->to->data_d);
@@ -1339,6 +1463,12 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
     it.tasks = gx.tasks_d;
     it.ntasks = gx.ntasks;
     it.max_pts = gx.max_pts;
+    it.group = g->index;
+    it.hfn = nullptr;
+    it.ffn = nullptr;
+    it.fid = -1;
+    it.idx32 = 0;
+    it.npts = 0;
     r.q.push_back(std::move(it));
     if (r.max_chain > 0 && (int)r.q.size() >= r.max_chain) ob2_flush();
   } else {
@@ -1474,6 +1604,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->ev_start = L->ev_end = nullptr;
   L->fuse_id = -1;  // the stub names its fused launcher after this call
   L->ffn = nullptr;
+  L->hfn = nullptr;
   if (L->npoints == 0) return 0;
 
   size_t red_bytes = 0;
@@ -1771,9 +1902,9 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
     snprintf(line, sizeof line,
              "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "
              "%lld tile launches, %lld multi-instance launches, %lld fused launches "
-             "(%lld loops)\n",
+             "(%lld loops), %lld halo transfers folded into loop launches\n",
              r.chains, r.graph_hits, r.graph_updates, r.tiles_run, r.multi_launches,
-             r.fused_launches, r.fused_loops);
+             r.fused_launches, r.fused_loops, r.hfused);
     s += line;
   }
   if (buf && n) {

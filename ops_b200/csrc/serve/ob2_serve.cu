@@ -6,15 +6,14 @@
 // grid of a few CTAs per SM walks the global unit index over all active
 // requests, finds the request by binary search in the prefix table, and works
 // on that request's tile.  One engine iteration:
-//   pois_pass     one pass of the single-reduction CG over every Poisson /
-//                 heat request: the iteration (p, s, x, r and w = A r with
-//                 per-tile (r, r), (w, r)), or the FP64 residual b - A x and
-//                 w = A r of a residual replacement
+//   pois_pw       p' = r + beta p, w = A p', per-tile (p', w)
+//   scalars_a     alpha per Poisson request
+//   pois_xr       x += alpha p' (FP64), r -= alpha w, per-tile (r, r); or
+//                 the FP64 residual b - A x
 //   adi_pre       right-hand side of the ADI step (adi/preproc_kernel.h)
 //   adi_x/y/z     constant-coefficient Thomas solves (z adds into u)
-//   scalars_b     per request: fixed-order sum of its tile partials, alpha,
-//                 beta, residual replacement and convergence; heat time
-//                 steps; ADI step count
+//   scalars_b     per request: fixed-order sum of its tile partials, beta,
+//                 residual replacement and convergence; ADI step count
 // All kernels read the work list from device memory, so one captured graph
 // of K iterations serves every batch composition.
 #include <cuda_runtime.h>
@@ -34,6 +33,7 @@ constexpr int TX = 32;
 constexpr int MAXA = OB2S_MAX_ACTIVE;
 constexpr int ADI_MAX_N = 192;  // x-solve tile: 32 lines x n points in shared memory
 constexpr int ADI_XL = 32;      // lines per x-solve unit
+// (OB2S_HEAT2D is declared in ops_b200_serve.h)
 constexpr int ADI_YZ = 4;       // planes per y/z-solve unit (CTA 32 x 4 lines)
 constexpr double kHeatRho = 1.0;  // heat requests: dt / h^2 of the implicit step
 
@@ -42,13 +42,12 @@ struct Req {
   int phase, done, outer, inner_it, iters;
   int max_inner, max_outer, steps, step;
   int par;  // p buffer parity
-  int newstep;  // heat: the next pass starts a time step (b = x)
+  int newstep;  // heat: the next residual pass starts a time step (b = x)
   double tol, inner_tol;
   double alpha, beta, gamma, gamma_in0, rr0, rel;
-  double diag, off;  // operator: diag x - off (sum of the 4 neighbours)
+  double diag, off;  // heat operator: diag x - off (sum of the 4 neighbours)
   double *x, *b, *part;
-  void *r[2], *w[2], *s[2], *p;
-  void *y;  // mixed mode: FP32 correction accumulator (NULL in FP64 mode)
+  void *r, *w, *p0, *p1;
   double *u, *du, *cp, *mm;
   double a_coef, lambda;
 };
@@ -88,56 +87,37 @@ __device__ __forceinline__ double hash_uniform(int seed, int i, int j, int k) {
 
 // ---------------------------------------------------------------- Poisson
 // CTA 32 x 8 threads; each thread handles RY consecutive rows, so a tile is
-// 32 x (8 RY) points.  Loads of out-of-range rows are clamped to the zero
-// halo row below the grid (always valid memory) and only the stores are
-// guarded, so the loads of all rows are issued before any store.
+// 32 x (8 RY) points.  Loads of out-of-range rows are clamped to the last
+// interior row (always valid memory) and only the stores are guarded, so the
+// loads of all RY rows are issued before any store.
 //
-// Poisson and heat requests: A x = diag x - off (sum of the 4 neighbours)
-// with a zero Dirichlet boundary (Poisson: diag 4, off 1; a backward-Euler
-// heat step: diag 1 + 4 rho, off rho), solved by conjugate gradients in the
-// single-reduction form of Chronopoulos and Gear ("s-step iterative methods
-// for symmetric linear systems", J. Comput. Appl. Math. 25, 1989): with
-// w = A r and s = A p carried along,
-//   p_i = r_i + beta_i p_{i-1}      s_i = w_i + beta_i s_{i-1}
-//   x_{i+1} = x_i + alpha_i p_i     r_{i+1} = r_i - alpha_i s_i
-//   w_{i+1} = A r_{i+1}             gamma = (r, r), delta = (w, r) at i+1
-//   beta_{i+1} = gamma_{i+1} / gamma_i
-//   alpha_{i+1} = gamma_{i+1} / (delta_{i+1} - beta_{i+1} gamma_{i+1} / alpha_i)
-// so that one pass over the vectors and one scalar kernel make an
-// iteration (the two-reduction form needs two passes and two scalar
-// kernels).  w_{i+1} needs r_{i+1} at the four neighbours: each thread forms
-// r_{i+1} = r_i - alpha (w_i + beta s_{i-1}) of its rows and of the rows above
-// and below itself, the warp's lanes exchange theirs by shuffles and the edge
-// lanes form their outer neighbours from memory with the same arithmetic, so
-// every value of r_{i+1} is computed identically wherever it is used.
-// r, w and s are double-buffered (read [par], written [par ^ 1]); p and the
-// iterate are updated in place (read only at their own point).
-//
-// Precision: the vectors r, w, s, p are stored in TI (FP32 in the mixed mode,
-// FP64 otherwise); every value is formed in FP64 from its stored inputs and
-// rounded once to TI; dot products accumulate in FP64.  The FP64 mode updates
-// the FP64 iterate x every iteration.  The mixed mode accumulates alpha p into
-// an FP32 correction y instead and folds y into the FP64 x at each residual
-// replacement (reliable updates with a low-precision accumulator, as in
-// mixed-precision Krylov solvers since Sleijpen and van der Vorst,
-// Computing 56, 1996): between replacements y holds only the correction since
-// the last fold, so its rounding shrinks with the error it corrects.  Per
-// point per iteration the mixed mode moves 40 bytes (r, w, s, p, y read and
-// written in FP32), the FP64 mode 80.
-// The recursive residual is replaced by b - A x computed in FP64 whenever it
-// has dropped by inner_tol since the last true residual or meets the
-// tolerance; the search directions p, s are kept.
+// Poisson and heat requests: conjugate gradients (the standard
+// two-reduction form) with the iterate x in FP64, the vectors r, w, p in TI
+// (FP32 in the mixed mode, FP64 otherwise) and every dot product accumulated
+// in FP64.  Poisson: A x = 4 x - (neighbours); heat (one backward-Euler step
+// per solve, dt / h^2 = rho): A x = (1 + 4 rho) x - rho (neighbours), b the
+// previous step's solution.  The recursive residual is replaced by the true
+// one, b - A x computed in FP64, whenever it has dropped by inner_tol since
+// the last true residual or meets the tolerance (reliable updates: the
+// search direction is kept, so the Krylov convergence of FP64 CG is kept
+// too; an FP32 iterate or an FP32 correction accumulated between
+// replacements needs far more iterations on fine grids: 10575 instead of
+// 5781 at 2048^2, measured).
 // Phases:
 //   0  start (and restart after a breakdown; for heat requests also the start
-//      of each time step, which first sets b = x): r = b - A (x + y) [pois_pass]
-//   4  w = A r, fold x += y, y = 0, (r, r), (w, r)   [pois_pass]; alpha_0
-//   2  CG iteration                                  [pois_pass]; alpha, beta
-//   3  replacement: r = b - A (x + y) in FP64        [pois_pass]
-//   5  as 4, then beta from the true (r, r), p and s kept
-// The scalar kernel (scalars_b) moves every request to its next phase.
+//      of each time step, which first sets b = x): r = b - A x in FP64
+//   2  CG iteration: p' = r + beta p, w = A p', (p', w)   [pois_pw]
+//                    alpha = gamma / (p', w)               [scalars_a]
+//                    x += alpha p', r -= alpha w, (r, r)   [pois_xr]
+//                    beta, gamma; replacement test         [scalars_b]
+//   3  replacement: r = b - A x in FP64, convergence test on it; beta from
+//      the true (r, r), p kept
+// p is double-buffered (p[par] read, p[par ^ 1] written by pois_pw), since
+// pois_pw forms p' of the stencil neighbours itself: w = A p' needs p' at
+// the neighbours, and recomputing r + beta p there avoids a separate pass.
 
 constexpr int CTA_Y = 8;
-constexpr int NPART = 2;  // partial sums per tile: (r, r) and (w, r)
+constexpr int NPART = 2;  // partial sums per tile: (p', w) and (r, r)
 
 // resident CTAs per SM the Poisson kernels are compiled for (register cap)
 #ifndef OB2S_MINB
@@ -168,174 +148,171 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (*sh)[32]) {
   __syncthreads();
 }
 
-// r_{i+1} at one point from the stored r_i, w_i, s_{i-1}: the one expression
-// every thread uses for it
-template <typename TI>
-__device__ __forceinline__ TI next_r(TI r, TI w, TI s, double alpha, double beta, TI &s_new) {
-  s_new = (TI)((double)w + beta * (double)s);
-  return (TI)((double)r - alpha * (double)s_new);
-}
-
-// one pass of a Poisson / heat request's current phase over the tile
+// p' = r + beta p and w = A p' over the tile, (p', w) per tile (phase 2)
 template <typename TI, int RY>
-__global__ void POIS_BOUNDS pois_pass(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[NPART][32];
+__global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
+  __shared__ double sh[1][32];
   const long long total = W->pois_pref[W->npois];
-  const unsigned full = 0xffffffffu;
   for (long long un = blockIdx.x; un < total; un += gridDim.x) {
     const int k = find_req(W->pois_pref, W->npois, un);
     const Req &q = R[W->pois_slot[k]];
-    const int ph = q.phase;
-    if (q.done) continue;  // uniform over the CTA
+    if (q.done || q.phase != 2) continue;  // uniform over the CTA
     const int t = (int)(un - W->pois_pref[k]);
     const int n = q.n, P = q.pitch;
-    const int lane = threadIdx.x;
-    const int i = (t % q.tiles_x) * TX + lane;
+    const int i = (t % q.tiles_x) * TX + threadIdx.x;
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
-    const bool inx = i < n;
-    const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
-    const double diag = q.diag, off = q.off;
-    const int cur = q.par, nxt = q.par ^ 1;
-    const bool mixed = q.y != nullptr;
-    double v[NPART] = {0.0, 0.0};
+    double v[1] = {0.0};
     if (j0 < n) {  // uniform over the warp (one threadIdx.y per warp)
-      // storage offsets of rows j0-1 .. j0+RY of column i, clamped into the
-      // array ((n + 2)^2 < 2^31 for n <= 32768)
-      int o[RY + 2];
+      const TI *rr = (const TI *)q.r;
+      const TI *pin = (const TI *)(q.par ? q.p1 : q.p0);
+      TI *pout = (TI *)(q.par ? q.p0 : q.p1);
+      TI *ww = (TI *)q.w;
+      const TI beta = (TI)q.beta;
+      const bool inx = i < n;
+      const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
+      const int lane = threadIdx.x;
+      // p' = r + beta p on rows j0-1 .. j0+RY of column i (storage rows
+      // clamped into the array; the halo rows and columns of r and p hold
+      // zeros); a lane past the right edge stands for the zero halo column
+      TI pc[RY + 2];
+      int o[RY + 2];  // (n + 2)^2 < 2^31 for n <= 32768
 #pragma unroll
-      for (int m = 0; m < RY + 2; m++) o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
+      for (int m = 0; m < RY + 2; m++) {
+        o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
+        pc[m] = inx ? rr[o[m]] + beta * pin[o[m]] : (TI)0;
+      }
+#pragma unroll
+      for (int m = 0; m < RY; m++) {
+        // west / east neighbours from the adjacent lanes; the warp's edge
+        // lanes form theirs from memory (the same arithmetic, same bits)
+        TI pw = __shfl_up_sync(0xffffffffu, pc[m + 1], 1);
+        TI pe = __shfl_down_sync(0xffffffffu, pc[m + 1], 1);
+        if (lane == 0) pw = rr[o[m + 1] - 1] + beta * pin[o[m + 1] - 1];
+        if (lane == TX - 1 && inx) pe = rr[o[m + 1] + 1] + beta * pin[o[m + 1] + 1];
+        if (!inx || j0 + m >= n) continue;
+        const TI c = pc[m + 1];
+        const TI a = q.kind == OB2S_HEAT2D
+                         ? (TI)q.diag * c - (TI)q.off * (pw + pe + pc[m] + pc[m + 2])
+                         : (TI)4 * c - pw - pe - pc[m] - pc[m + 2];
+        pout[o[m + 1]] = c;
+        ww[o[m + 1]] = a;
+        v[0] += (double)c * (double)a;
+      }
+    }
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) q.part[NPART * t] = v[0];
+  }
+}
+
+// phase 2: x += alpha p' (FP64), r -= alpha w, (r, r); phases 0, 3:
+// r = b - A x in FP64 and its (r, r)
+template <typename TI, int RY>
+__global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
+  __shared__ double sh[2][32];
+  const long long total = W->pois_pref[W->npois];
+  for (long long un = blockIdx.x; un < total; un += gridDim.x) {
+    const int k = find_req(W->pois_pref, W->npois, un);
+    const Req &q = R[W->pois_slot[k]];
+    if (q.done) continue;  // uniform over the CTA
+    const int ph = q.phase;
+    const int t = (int)(un - W->pois_pref[k]);
+    const int n = q.n, P = q.pitch;
+    const int i = (t % q.tiles_x) * TX + threadIdx.x;
+    const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
+    double v[2] = {0.0, 0.0};
+    if (i < n && j0 < n) {
+      int o[RY];  // (n + 2)^2 < 2^31 for n <= 32768
+#pragma unroll
+      for (int m = 0; m < RY; m++) o[m] = (min(j0 + m, n - 1) + 1) * P + (i + 1);
+      TI *rr = (TI *)q.r;
+      double *x = q.x;
       if (ph == 2) {
-        const TI *r = (const TI *)q.r[cur], *w = (const TI *)q.w[cur];
-        const TI *s = (const TI *)q.s[cur];
-        TI *r1 = (TI *)q.r[nxt], *w1 = (TI *)q.w[nxt], *s1 = (TI *)q.s[nxt];
-        TI *pp = (TI *)q.p;
-        const double alpha = q.alpha, beta = q.beta;
-        TI rn[RY + 2], sn[RY + 2];
+        const TI *pn = (const TI *)(q.par ? q.p0 : q.p1);  // written by pois_pw
+        const TI *ww = (const TI *)q.w;
+        const double alpha64 = q.alpha;
+        const TI alpha = (TI)q.alpha;
+        double xv[RY];
+        TI rv[RY];
 #pragma unroll
-        for (int m = 0; m < RY + 2; m++) {
-          rn[m] = (TI)0;
-          sn[m] = (TI)0;
-          if (inx) rn[m] = next_r<TI>(r[o[m]], w[o[m]], s[o[m]], alpha, beta, sn[m]);
+        for (int m = 0; m < RY; m++) {
+          const TI pv = pn[o[m]];
+          xv[m] = x[o[m]] + alpha64 * (double)pv;
+          rv[m] = rr[o[m]] - alpha * ww[o[m]];
         }
 #pragma unroll
         for (int m = 0; m < RY; m++) {
-          const int oc = o[m + 1];
-          TI rw = __shfl_up_sync(full, rn[m + 1], 1);
-          TI re = __shfl_down_sync(full, rn[m + 1], 1);
-          TI dummy;
-          if (lane == 0) rw = next_r<TI>(r[oc - 1], w[oc - 1], s[oc - 1], alpha, beta, dummy);
-          if (lane == TX - 1 && inx)
-            re = next_r<TI>(r[oc + 1], w[oc + 1], s[oc + 1], alpha, beta, dummy);
-          if (!inx || j0 + m >= n) continue;
-          const TI rc = rn[m + 1];
-          const TI wn = (TI)(diag * (double)rc -
-                             off * ((double)rw + (double)re + (double)rn[m] + (double)rn[m + 2]));
-          const TI pn = (TI)((double)r[oc] + beta * (double)pp[oc]);
-          if (mixed) {
-            TI *y = (TI *)q.y;
-            y[oc] = (TI)((double)y[oc] + alpha * (double)pn);
+          if (j0 + m >= n) continue;
+          x[o[m]] = xv[m];
+          rr[o[m]] = rv[m];
+          v[0] += (double)rv[m] * (double)rv[m];
+        }
+      } else {
+        double *b = q.b;
+        double res[RY];
+#pragma unroll
+        for (int m = 0; m < RY; m++) {
+          const int e = o[m];
+          if (q.kind == OB2S_HEAT2D) {
+            const double c = x[e];
+            double bv = b[e];
+            if (q.newstep) {  // a new time step: its right-hand side is the last solution
+              bv = c;
+              if (j0 + m < n) {
+                b[e] = bv;
+                v[1] += bv * bv;  // ||b||^2: the step's residuals are relative to it
+              }
+            }
+            res[m] = bv - (q.diag * c - q.off * (x[e - 1] + x[e + 1] + x[e - P] + x[e + P]));
           } else {
-            q.x[oc] = q.x[oc] + alpha * (double)pn;
+            res[m] = b[e] - (4.0 * x[e] - x[e - 1] - x[e + 1] - x[e - P] - x[e + P]);
           }
-          pp[oc] = pn;
-          r1[oc] = rc;
-          s1[oc] = sn[m + 1];
-          w1[oc] = wn;
-          v[0] += (double)rc * (double)rc;
-          v[1] += (double)wn * (double)rc;
         }
-      } else if (ph == 0 || ph == 3) {
-        // r = b - A (x + y) in FP64 (heat: b = x first at a new time step)
-        const double *x = q.x;
-        const TI *y = (const TI *)q.y;
-        double xs[RY + 2];
-#pragma unroll
-        for (int m = 0; m < RY + 2; m++)
-          xs[m] = inx ? x[o[m]] + (mixed ? (double)y[o[m]] : 0.0) : 0.0;
-        TI *r = (TI *)q.r[cur];
 #pragma unroll
         for (int m = 0; m < RY; m++) {
-          const int oc = o[m + 1];
-          double xw = __shfl_up_sync(full, xs[m + 1], 1);
-          double xe = __shfl_down_sync(full, xs[m + 1], 1);
-          if (lane == 0) xw = x[oc - 1] + (mixed ? (double)y[oc - 1] : 0.0);
-          if (lane == TX - 1 && inx) xe = x[oc + 1] + (mixed ? (double)y[oc + 1] : 0.0);
-          if (!inx || j0 + m >= n) continue;
-          double bv = q.b[oc];
-          if (q.newstep) {
-            bv = xs[m + 1];
-            q.b[oc] = bv;
-          }
-          const double ax = diag * xs[m + 1] - off * (xw + xe + xs[m] + xs[m + 2]);
-          r[oc] = (TI)(bv - ax);
-        }
-      } else {  // phases 4, 5: w = A r, fold the correction, (r, r), (w, r)
-        const TI *r = (const TI *)q.r[cur];
-        TI *w = (TI *)q.w[cur];
-        TI rs[RY + 2];
-#pragma unroll
-        for (int m = 0; m < RY + 2; m++) rs[m] = inx ? r[o[m]] : (TI)0;
-#pragma unroll
-        for (int m = 0; m < RY; m++) {
-          const int oc = o[m + 1];
-          TI rw = __shfl_up_sync(full, rs[m + 1], 1);
-          TI re = __shfl_down_sync(full, rs[m + 1], 1);
-          if (lane == 0) rw = r[oc - 1];
-          if (lane == TX - 1 && inx) re = r[oc + 1];
-          if (!inx || j0 + m >= n) continue;
-          const TI rc = rs[m + 1];
-          const TI wn = (TI)(diag * (double)rc -
-                             off * ((double)rw + (double)re + (double)rs[m] + (double)rs[m + 2]));
-          w[oc] = wn;
-          if (mixed) {
-            TI *y = (TI *)q.y;
-            q.x[oc] = q.x[oc] + (double)y[oc];
-            y[oc] = (TI)0;
-          }
-          v[0] += (double)rc * (double)rc;
-          v[1] += (double)wn * (double)rc;
+          if (j0 + m >= n) continue;
+          rr[o[m]] = (TI)res[m];
+          v[0] += res[m] * res[m];
         }
       }
     }
-    if (ph == 2 || ph == 4 || ph == 5) {  // uniform over the CTA
-      block_sum<NPART>(v, sh);
-      if (threadIdx.x == 0 && threadIdx.y == 0) {
-        q.part[NPART * t] = v[0];
-        q.part[NPART * t + 1] = v[1];
-      }
+    block_sum<2>(v, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      q.part[NPART * t + 1] = v[0];
+      // column 0 is free in phase 0 (pois_pw did not run): ||b||^2 of a new
+      // heat time step
+      if (ph == 0 && q.newstep) q.part[NPART * t] = v[1];
     }
   }
 }
 
-// per-request fixed-order sums of the two partial columns
-__device__ __forceinline__ void request_sums(const Req &q, double (*sh)[32], double &g,
-                                             double &d) {
-  double v[NPART] = {0.0, 0.0};
-  for (int t = threadIdx.x; t < q.tiles; t += blockDim.x) {
-    v[0] += q.part[NPART * t];
-    v[1] += q.part[NPART * t + 1];
-  }
-  block_sum<NPART>(v, sh);
-  g = v[0];
-  d = v[1];
+// per-request fixed-order sum of one partial column
+__device__ __forceinline__ double request_sum(const Req &q, int col, double (*sh)[32]) {
+  double v[1] = {0.0};
+  for (int t = threadIdx.x; t < q.tiles; t += blockDim.x) v[0] += q.part[NPART * t + col];
+  block_sum<1>(v, sh);
+  return v[0];
 }
 
-// after a converged solve: the next heat time step, or done
-__device__ __forceinline__ void finish_solve(Req &q) {
-  if (q.kind == OB2S_HEAT2D && q.step + 1 < q.steps) {
-    q.step++;
-    q.newstep = 1;
-    q.outer = 0;
-    q.phase = 0;
+// alpha = gamma / (p', w) for requests in phase 2
+__global__ void __launch_bounds__(256) scalars_a(const Work *__restrict__ W, Req *R) {
+  __shared__ double sh[1][32];
+  const int b = blockIdx.x;
+  if (b >= W->npois) return;
+  Req &q = R[W->pois_slot[b]];
+  if (q.done || q.phase != 2) return;
+  const double pw = request_sum(q, 0, sh);
+  if (threadIdx.x != 0) return;
+  if (!(pw > 0.0)) {  // breakdown: pois_xr computes the true residual and
+    q.phase = 0;       // scalars_b restarts from it with beta = 0
     return;
   }
-  q.done = 1;
+  q.alpha = q.gamma / pw;
 }
 
-// Every request's next phase (thread 0 of one CTA per request slot; CTAs
-// [MAXA, MAXA + nadi) advance the ADI requests' step counts).
+// (r, r) step of every Poisson request; CTAs [MAXA, MAXA + nadi) advance
+// the ADI requests' step counts
 __global__ void __launch_bounds__(256) scalars_b(const Work *__restrict__ W, Req *R) {
-  __shared__ double sh[NPART][32];
+  __shared__ double sh[1][32];
   const int b = blockIdx.x;
   if (b >= MAXA) {
     const int k = b - MAXA;
@@ -351,57 +328,45 @@ __global__ void __launch_bounds__(256) scalars_b(const Work *__restrict__ W, Req
   Req &q = R[W->pois_slot[b]];
   if (q.done) return;
   const int ph = q.phase;
-  if (ph == 0 || ph == 3) {  // r written; w, the fold and the dots next
-    if (threadIdx.x == 0) {
-      q.newstep = 0;
-      q.phase = ph == 0 ? 4 : 5;
-    }
-    return;
-  }
-  double g, dl;
-  request_sums(q, sh, g, dl);
+  const bool newstep = ph == 0 && q.newstep;  // uniform over the CTA
+  const double g = request_sum(q, 1, sh);
+  const double bb = newstep ? request_sum(q, 0, sh) : 0.0;
   if (threadIdx.x != 0) return;
-  if (ph == 4 || ph == 5) {  // true residual: g = (r, r), dl = (w, r)
-    if (q.outer == 0) q.rr0 = g;
+  if (ph == 0 || ph == 3) {  // g = (b - A x, b - A x) in FP64
+    if (newstep) {  // heat: relative to the step's right-hand side
+      q.rr0 = bb;
+      q.newstep = 0;
+    } else if (q.outer == 0) {
+      q.rr0 = g;  // Poisson starts from x = 0: (b, b)
+    }
     q.outer++;
     q.rel = q.rr0 > 0.0 ? sqrt(g / q.rr0) : 0.0;
-    if (q.rel <= q.tol || q.outer > q.max_outer || q.iters >= q.max_inner || g == 0.0) {
-      finish_solve(q);
+    if (q.rel <= q.tol || q.outer > q.max_outer || q.iters >= q.max_inner) {
+      if (q.kind == OB2S_HEAT2D && q.rel <= q.tol && q.step + 1 < q.steps) {
+        q.step++;  // next backward-Euler step, from this solution
+        q.newstep = 1;
+        q.outer = 0;
+        q.phase = 0;
+        return;
+      }
+      q.done = 1;
       return;
     }
-    double beta = 0.0, den = dl;
-    if (ph == 5) {
-      beta = g / q.gamma;
-      den = dl - beta * g / q.alpha;
-    }
-    if (!(den > 0.0)) {  // breakdown: start again from the true residual
-      q.phase = 0;
-      return;
-    }
-    q.beta = beta;
-    q.alpha = g / den;
+    q.beta = ph == 0 ? 0.0 : g / q.gamma;
     q.gamma = g;
     q.gamma_in0 = g;
     q.phase = 2;
     return;
   }
-  // phase 2: recursive (r, r) and (w, r) of the new residual
   q.iters++;
   q.par ^= 1;
   const double drop = sqrt(g / q.gamma_in0);
   const double relr = q.rr0 > 0.0 ? sqrt(g / q.rr0) : 0.0;
   if (drop <= q.inner_tol || relr <= q.tol || q.iters >= q.max_inner || g == 0.0) {
-    q.phase = 3;  // gamma and alpha stay those of the step just taken
+    q.phase = 3;  // gamma stays the previous (r, r) for beta
     return;
   }
-  const double beta = g / q.gamma;
-  const double den = dl - beta * g / q.alpha;
-  if (!(den > 0.0)) {
-    q.phase = 3;  // loss of positivity: replace the residual and go on from it
-    return;
-  }
-  q.beta = beta;
-  q.alpha = g / den;
+  q.beta = g / q.gamma;
   q.gamma = g;
 }
 
@@ -585,9 +550,7 @@ OB2_API size_t ob2s_request_bytes(int mode, int kind, int n) {
   if (kind == OB2S_POISSON2D || kind == OB2S_HEAT2D) {
     const size_t p = (size_t)(n + 2) * (n + 2);
     const size_t tiles = (size_t)((n + 31) / 32) * (size_t)((n + 7) / 8);  // at the smallest tile
-    // x, b (FP64); r, w, s (two buffers each) and p; y in the mixed mode
-    const size_t vec = 7 + (mode == OB2S_MIXED ? 1 : 0);
-    return p * (16 + vec * elem_inner(mode)) + 8 * NPART * tiles + 4096;
+    return p * (16 + 4 * elem_inner(mode)) + 8 * NPART * tiles + 4096;
   }
   return (size_t)n * n * n * 16 + (size_t)n * 16 + 4096;
 }
@@ -599,8 +562,10 @@ static int launch_iteration(ob2s_engine *e, int variant) {
   int k = 0;
   if (variant & 1) {
     const int g = e->sms * e->pois_ctas_per_sm;
-    pois_pass<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
-    k += 1;
+    pois_pw<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
+    scalars_a<<<MAXA, 256, 0, e->st>>>(e->W_d, e->R_d);
+    pois_xr<TI, RY><<<g, dim3(TX, CTA_Y), 0, e->st>>>(e->W_d, e->R_d);
+    k += 3;
   }
   if (variant & 2) {
     adi_pre<<<e->sms * 8, dim3(32, 8), 0, e->st>>>(e->W_d, e->R_d);
@@ -654,7 +619,7 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
   }
   {
     // persistent grids: as many CTAs as can be resident at once
-    int nb = 0;
+    int nb = 0, nb2 = 0;
     const bool mixed = mode == OB2S_MIXED;
     auto occ = [&](const void *f) {
       int b = 0;
@@ -663,15 +628,17 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
     };
     switch (tile_y) {
       case 8:
-        nb = occ(mixed ? (const void *)pois_pass<float, 1> : (const void *)pois_pass<double, 1>);
+        nb = occ(mixed ? (const void *)pois_pw<float, 1> : (const void *)pois_pw<double, 1>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 1> : (const void *)pois_xr<double, 1>);
         break;
       case 16:
-        nb = occ(mixed ? (const void *)pois_pass<float, 2> : (const void *)pois_pass<double, 2>);
+        nb = occ(mixed ? (const void *)pois_pw<float, 2> : (const void *)pois_pw<double, 2>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 2> : (const void *)pois_xr<double, 2>);
         break;
       default:
-        nb = occ(mixed ? (const void *)pois_pass<float, 4> : (const void *)pois_pass<double, 4>);
+        nb = occ(mixed ? (const void *)pois_pw<float, 4> : (const void *)pois_pw<double, 4>);
+        nb2 = occ(mixed ? (const void *)pois_xr<float, 4> : (const void *)pois_xr<double, 4>);
     }
-    const int nb2 = nb;
     e->pois_ctas_per_sm = std::max(1, std::min(nb, nb2));
   }
   e->R.assign(MAXA, Req());
@@ -754,25 +721,20 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
     q.tiles = q.tiles_x * ((n + e->tile_y - 1) / e->tile_y);
     const size_t p = (size_t)q.pitch * q.pitch;
     const size_t ei = elem_inner(e->mode);
-    // the layout ob2s_request_bytes counts (each array rounded up to 256
-    // bytes: within its 4 KB slack); every array starts zeroed
+    // the layout ob2s_request_bytes counts (seven arrays, each rounded up to
+    // 256 bytes: within its 4 KB slack)
     q.x = (double *)take(p * 8);
     q.b = (double *)take(p * 8);
-    for (int c = 0; c < 2; c++) {
-      q.r[c] = take(p * ei);
-      q.w[c] = take(p * ei);
-      q.s[c] = take(p * ei);
-    }
-    q.p = take(p * ei);
-    q.y = e->mode == OB2S_MIXED ? take(p * ei) : nullptr;
+    q.r = take(p * ei);
+    q.w = take(p * ei);
+    q.p0 = take(p * ei);
+    q.p1 = take(p * ei);
     q.part = (double *)take((size_t)8 * NPART * q.tiles);
-    if (kind == OB2S_HEAT2D) {  // backward Euler, dt = h^2: (1 + 4) x - (neighbours)
+    if (kind == OB2S_HEAT2D) {  // backward Euler: (1 + 4 rho) x - rho (neighbours)
       q.diag = 1.0 + 4.0 * kHeatRho;
       q.off = kHeatRho;
       q.steps = steps;
-    } else {
-      q.diag = 4.0;
-      q.off = 1.0;
+      q.newstep = 1;  // the first step's right-hand side is u0 (= x)
     }
     q.tol = e->tol;
     q.inner_tol = e->inner_tol;
@@ -790,7 +752,7 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
   }
   if (kind == OB2S_POISSON2D) {
     pois_init<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.b, n, q.pitch, seed);
-  } else if (kind == OB2S_HEAT2D) {  // u0 is the first right-hand side and first guess
+  } else if (kind == OB2S_HEAT2D) {  // u0 is the first right-hand side and guess
     heat_init<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.b, q.x, n, q.pitch, seed);
   } else {
     q.lambda = 1.0;

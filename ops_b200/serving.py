@@ -184,17 +184,15 @@ def make_stream(count: int, rate: float, seed: int, adi_frac: float = 0.3,
 
 
 def request_bytes_moved(r: Request, mode: int) -> float:
-    """Algorithmic bytes of a finished request.  Poisson / heat: per CG
-    iteration the single-reduction pass reads and writes r, w = A r, s = A p,
-    p and the iterate (mixed: FP32 vectors and the FP32 correction, 40 B per
-    point; FP64: 80 B); per residual replacement the FP64 residual pass reads
-    x, b and the correction and writes r, and the w = A r pass reads r and
-    writes w and folds the correction into x (mixed 24 + 32 B per point, FP64
-    24 + 16 B).  ADI: 72 B per point per step (preproc reads u and writes du,
-    the x and y solves read and write du, the z solve reads du and updates
-    u)."""
+    """Algorithmic bytes of a finished request.  Poisson / heat, per CG
+    iteration: p' = r + beta p and w = A p' read r and p and write p' and w;
+    the update pass reads p' and w and updates x (FP64) and r (FP64: 80 B
+    per point; mixed, with FP32 r, w, p and the FP64 x: 48 B); per residual
+    replacement the FP64 residual pass reads x and b and writes r (24 B).
+    ADI: 72 B per point per step (preproc reads u and writes du, the x and y
+    solves read and write du, the z solve reads du and updates u)."""
     if r.kind in (POISSON2D, HEAT2D):
-        per, outer = (40.0, 56.0) if mode == MIXED else (80.0, 40.0)
+        per, outer = (48.0, 24.0) if mode == MIXED else (80.0, 24.0)
         return r.n * r.n * (per * r.iterations + outer * (r.outer + 1))
     return r.n ** 3 * 72.0 * r.steps
 

@@ -931,6 +931,24 @@ class Translator:
             w("  %s<RESTRICT, IDX32>(m.p[it], blockIdx.x, blockIdx.y, blockIdx.z - it * m.gz);" %
               BF)
             w("}")
+            # the same with a halo group folded in: each CTA first copies the
+            # group's cells in its footprint (tile widened by the stencil
+            # reach), then runs the loop; unrestricted pointers, since the
+            # loop reads cells this launch writes
+            w("template <bool IDX32>")
+            w("__global__ void __launch_bounds__(%s) %sH(const __grid_constant__ %sM m,"
+              " const __grid_constant__ ob2_hfuse h) {" % (lb, K, P))
+            w("  const unsigned it = blockIdx.z / m.gz, bz = blockIdx.z - it * m.gz;")
+            w("  const %s &p = m.p[it];" % P)
+            w("  const int x0 = p.lo0 + (int)(blockIdx.x * blockDim.x);")
+            w("  const int y0 = p.lo1 + (int)(blockIdx.y * blockDim.y) * %d;" % py)
+            w("  const int z0 = p.lo2 + (int)(bz * blockDim.z);")
+            w("  ob2::hfuse_prologue(h, (int)it, x0, min(x0 + (int)blockDim.x, p.hi0), y0,"
+              " min(y0 + (int)blockDim.y * %d, p.hi1), z0, min(z0 + (int)blockDim.z, p.hi2));" %
+              py)
+            w("  __syncthreads();")
+            w("  %s<false, IDX32>(p, blockIdx.x, blockIdx.y, bz);" % BF)
+            w("}")
         # launchers: the runtime launches a loop now or, in lazy mode, later
         # (possibly once per tile, possibly inside a graph capture)
         LN = "ob2l_" + loop.stub[len("ops_par_loop_"):]
@@ -946,6 +964,19 @@ class Translator:
                 w("  m.gz = g[2];")
                 w("  %sM<%s, %s><<<dim3(g[0], g[1], g[2] * n), dim3(b[0], b[1], b[2]), 0,"
                   " (cudaStream_t)st>>>(m);" % (K, rs, ix))
+                w("  return (int)cudaGetLastError();")
+                w("}")
+        HN = "ob2h_" + loop.stub[len("ops_par_loop_"):]
+        if not reds:
+            for ix in ("false", "true"):
+                w("static int %s_%s(const void *const *prm, int n, const unsigned *g,"
+                  " const unsigned *b, const ob2_hfuse *h, void *st) {" % (HN, ix[0]))
+                w("  if (n < 1 || n > OB2_MULTI_MAX) return (int)cudaErrorInvalidValue;")
+                w("  %sM m;" % P)
+                w("  for (int k = 0; k < n; k++) m.p[k] = *(const %s *)prm[k];" % P)
+                w("  m.gz = g[2];")
+                w("  %sH<%s><<<dim3(g[0], g[1], g[2] * n), dim3(b[0], b[1], b[2]), 0,"
+                  " (cudaStream_t)st>>>(m, *h);" % (K, ix))
                 w("  return (int)cudaGetLastError();")
                 w("}")
         for rs, ix in (("false", "false"), ("false", "true"), ("true", "false"), ("true", "true")):
@@ -1027,6 +1058,7 @@ class Translator:
         if not reds:
             w("  L.fuse_id = %d;" % len(self.fuse_items))
             w("  L.ffn = ob2f_launch;")
+            w("  L.hfn = L.idx32 ? %s_t : %s_f;" % (HN, HN))
             self.fuse_items.append((P, "ob2b_" + loop.stub[len("ops_par_loop_"):]))
         w("  ob2_launch(&L, fn, mfn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")

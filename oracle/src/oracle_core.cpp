@@ -435,14 +435,22 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
       for (int c = 0; c < h->from->dim; c++) {
         char *src = elem_ptr(h->from, fs, c);
         char *dst = elem_ptr(h->to, ts, c);
+        // mixed types: each value converted to the destination type
+        // (ops_host_singlenode.cpp:279-300 / 398-420 go through the smaller
+        // of the two types, the same value as the direct conversion)
         if (h->from->type_size == h->to->type_size) {
           memcpy(dst, src, h->from->type_size);
-        } else if (h->from->type_size == 8 && h->to->type_size == 4) {
-          *(float *)dst = (float)*(double *)src;
-        } else if (h->from->type_size == 4 && h->to->type_size == 8) {
-          *(double *)dst = (double)*(float *)src;
         } else {
-          throw OPSException(OPS_NOT_IMPLEMENTED, "Error: unsupported mixed halo types");
+          double v;
+          const int fs2 = h->from->type_size, ts2 = h->to->type_size;
+          if (fs2 == 8) v = *(double *)src;
+          else if (fs2 == 4) v = (double)*(float *)src;
+          else if (fs2 == 2) v = (double)*(half *)src;
+          else throw OPSException(OPS_NOT_IMPLEMENTED, "Error: unsupported mixed halo types");
+          if (ts2 == 8) *(double *)dst = v;
+          else if (ts2 == 4) *(float *)dst = (float)v;
+          else if (ts2 == 2) *(half *)dst = (half)v;
+          else throw OPSException(OPS_NOT_IMPLEMENTED, "Error: unsupported mixed halo types");
         }
       }
     }

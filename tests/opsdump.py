@@ -10,7 +10,7 @@ from typing import Dict, Tuple
 import numpy as np
 
 _NP = {"double": np.float64, "float": np.float32, "int": np.int32, "long long": np.int64,
-       "ll": np.int64}
+       "ll": np.int64, "half": np.float16}
 
 
 def read_dump(path: str, mmap: bool = False) -> Dict[str, Tuple[dict, np.ndarray]]:

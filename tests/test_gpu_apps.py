@@ -192,6 +192,10 @@ REF_APPS = [
     ("ref_adi_burger", [], "roundoff", "Successful exit from OPS"),
     ("ref_adi_burger3d", [], "roundoff", "Successful exit from OPS"),
     ("ref_tti", ["24", "20", "16"], "exact", "ops_NaNcheck_core called for ut0"),
+    # half-precision dats (ACC<half>): IEEE binary16 arithmetic on both sides
+    ("ref_halfprecision", [], "half", "This run is considered PASSED"),
+    ("ref_lbm", [], "exact", "Test PASSED"),
+    ("ref_tiling_fix", [], "exact", ""),
 ]
 
 
@@ -228,6 +232,14 @@ def test_more_reference_apps_match_oracle(tmp_path, name, args, mode, text):
         check_dumps(dumps["b200"], dumps["oracle"], tol=1e-12, float_tol=1e-6, floor_frac=1.0)
     elif mode == "libm":
         check_dumps(dumps["b200"], dumps["oracle"], tol=1e-6, float_tol=1e-5, floor_frac=1.0)
+    elif mode == "half":
+        # every binary16 operation is correctly rounded on both sides (the
+        # host's _Float16 rounds each operation), so values agree; the
+        # boundary values come from sin / exp in FP64 rounded to binary16,
+        # where a last-ulp difference of libm may flip one rounding: at most
+        # one binary16 ulp (2^-10 relative)
+        diffs = compare(dumps["b200"], dumps["oracle"])
+        assert max(diffs.values()) <= 2.0 ** -10, diffs
 
 
 @pytest.mark.parametrize("solver", ["tl_use_jacobi", "tl_use_cg", "tl_use_chebyshev"])
@@ -271,6 +283,14 @@ def test_reference_mb_trid_regression_on_b200():
     two blocks, an ops_tridsolver_params per block, everything deleted again):
     a regression case for a crash in the reference; it must run to the end."""
     run_exe("ref_mb_trid", "b200", cwd=tempfile.mkdtemp(prefix="mbtrid_"))
+
+
+def test_reference_mb_shsgc_on_b200():
+    """The reference's mb_shsgc (shock-capturing shsgc written with the
+    original OPS_ACCn kernel API, the Max_datatransfer variant) built
+    unchanged: its own check of the post-shock error passes."""
+    out = run_exe("ref_mb_shsgc", "b200", cwd=tempfile.mkdtemp(prefix="mbshsgc_"))
+    assert "PASSED" in out, out[-1500:]
 
 
 def test_reference_cloverleaf3d_known_answer_on_b200():

@@ -69,11 +69,24 @@ def test_cloverleaf_3840_matches_reference_openmp(tmp_path):
 
 @pytest.mark.parametrize("prec", ["64", "32"])
 def test_adi_256_matches_oracle(prec, tmp_path):
+    """The state u per element (1e-12 FP64, 1e-6 FP32 storage); du, the
+    right-hand side the three solves overwrite, relative to its field's scale
+    (1e-12 of max|du|): the chunked Thomas/PCR elimination rounds in another
+    order than the oracle's sequential Thomas sweep, which shows per element
+    on du's near-zero values (5e-12 of the element at 1e-3 of the scale,
+    i.e. 5e-15 of the scale) but stays at round-off of the field."""
     args = ["-n=256", "-steps=3", "-prec=" + prec]
     try:
         gout, gd = run_app("adi3d", "b200", args, dump=True)
         cout, cd = run_app("adi3d", "oracle", args, dump=True)
-        check(gd, cd)
+        diffs = compare(gd, cd, mmap=True, skip=("du_",))
+        meta = read_dump(cd, mmap=True)
+        for name, d in diffs.items():
+            assert d <= (1e-6 if meta[name][0]["type"] == "float" else 1e-12), (name, d)
+        dd = compare(gd, cd, mmap=True, floor_frac=1.0)
+        for name, d in dd.items():
+            if name.startswith("du_"):
+                assert d <= (1e-6 if meta[name][0]["type"] == "float" else 1e-12), (name, d)
     finally:
         for p in (locals().get("gd"), locals().get("cd")):
             if p and os.path.exists(p):

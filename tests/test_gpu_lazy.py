@@ -56,6 +56,26 @@ def test_lazy_matches_eager(app, args, mode):
     assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
 
 
+@pytest.mark.parametrize("args", [["-nb=2", "-n=61", "-sweeps=25", "-check=5"],
+                                  ["-nb=2", "-n=256", "-sweeps=40", "-check=10"]])
+def test_halo_transfers_fold_into_the_consuming_launch(args):
+    """The multi-block Jacobi: every sweep's ops_halo_transfer is folded into
+    the launch of the four blocks' Jacobi loop (each CTA copies the halo
+    cells its stencil reads, then computes); every dat equals eager
+    execution bit for bit, and the same with folding switched off."""
+    eo, ed = run_app("poisson_mb", "b200", args, dump=True, env=EAGER)
+    lo, ld = run_app("poisson_mb", "b200", args, dump=True, env={"OPS_B200_LAZY": "1"})
+    no, nd = run_app("poisson_mb", "b200", args, dump=True,
+                     env={"OPS_B200_LAZY": "1", "OPS_B200_HFUSE": "0"})
+    sweeps = int(args[2].split("=")[1])
+    folded = int(re.search(r"(\d+) halo transfers folded", lo).group(1))
+    assert folded >= sweeps - sweeps // int(args[3].split("=")[1])
+    assert int(re.search(r"(\d+) halo transfers folded", no).group(1)) == 0
+    same(ld, ed)
+    same(nd, ed)
+    assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
+
+
 @pytest.mark.parametrize("mode", ["lazy_graphs", "tiled_graphs", "tiled_cache"])
 def test_cloverleaf_lazy_matches_eager(tmp_path, mode):
     ensure("clover_step", "b200")
