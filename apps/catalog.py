@@ -234,7 +234,9 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
         objs = []
         for p in paths:
             o = os.path.join(out, os.path.basename(p) + ".o")
-            cmd = ["g++", "-O2", "-g", "-std=c++17", "-fPIC", "-w", *inc]
+            # binary16 (`half`) arithmetic rounded after every operation, as
+            # CUDA's __half does (GCC would otherwise evaluate it in float)
+            cmd = ["g++", "-O2", "-g", "-std=c++17", "-fPIC", "-w", "-fexcess-precision=16", *inc]
             if name == "clover_step" and os.path.basename(p) == "clover_leaf.cpp":
                 cmd += extra_defs
             if shared and name != "clover_step":
@@ -294,7 +296,10 @@ def build(name: str, flavour: str, shared: bool = False, force: bool = False) ->
             objs.append(o)
         link = ["g++", "-fopenmp", "-o", target, *pre_objs, *objs, lib]
         if flavour == "ref_cuda":
+            # libops_cuda reads GPU power counters through NVML
+            # (makefiles/Makefile.cuda:5): the driver's libnvidia-ml at run time
             link += ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart", "-lcurand",
+                     "-L" + os.path.join(CUDA_HOME, "lib64", "stubs"), "-lnvidia-ml",
                      "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")]
         if shared:
             link[1:1] = ["-shared", "-Wl,-Bsymbolic"]

@@ -126,6 +126,14 @@ __device__ __forceinline__ void reset_counter(unsigned int *counter) {
   if (t == 0) *counter = 0u;
 }
 
+/* CTA tile of the temporal-blocking kernels (ob2_tblock, ops_b200_loop.h) */
+#ifndef OB2_TB_TX
+#define OB2_TB_TX 64
+#endif
+#ifndef OB2_TB_TY
+#define OB2_TB_TY 16
+#endif
+
 /* ---- halo group folded into a loop launch (ob2_hfuse, ops_b200_loop.h) ----
  * Copies the cells of the folded group that lie in this CTA's footprint: the
  * CTA's tile [x0,x1) x [y0,y1) x [z0,z1) in loop coordinates widened by the

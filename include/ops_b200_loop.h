@@ -70,6 +70,29 @@ typedef struct ob2_hfuse {
 typedef int (*ob2_hlauncher)(const void *const *params, int n, const unsigned *grid,
                              const unsigned *block, const ob2_hfuse *h, void *stream);
 
+/* Shared-memory temporal blocking of a chain of sweeps (the GPU form of the
+ * reference's loop-chain tiling, ops_lazy.cpp:380-1187): consecutive queued
+ * instances of one 2D loop that ping-pong two dats -- sweep k reads dat X
+ * through a stencil of reach at most 1 and writes dat Y at the centre,
+ * sweep k+1 the other way round, everything else equal -- run `steps` sweeps
+ * in one launch.  Each CTA loads its tile widened by `steps` into shared
+ * memory (X, and Y outside the loop range), runs the sweeps there on
+ * shrinking regions with the loop's own point function, and writes the
+ * tile back: Y's new values in place, X's into X's spare buffer (`spare`:
+ * the view base of arg s in it), which then becomes X's storage (no CTA
+ * writes X while another may still read it).  The CTAs on the range edge
+ * also copy X's points outside the range (storage box sx0..sx1 x sy0..sy1
+ * in loop coordinates) into the spare.  Every point is computed by the same
+ * code on the same values as sweep by sweep, so results are identical. */
+#define OB2_TB_MAX 8
+typedef struct ob2_tblock {
+  int steps;       /* sweeps in this launch, 2..OB2_TB_MAX */
+  int s;           /* argument index of X (the stencil-read dat of the first sweep) */
+  char *spare;     /* view base of argument s in X's spare buffer */
+  int sx0, sx1, sy0, sy1;
+} ob2_tblock;
+typedef int (*ob2_tlauncher)(const void *params, const ob2_tblock *t, void *stream);
+
 typedef struct ob2_loop {
   const char *name;
   int kernel_index;  /* timing-table slot */
@@ -104,6 +127,12 @@ typedef struct ob2_loop {
                                stub before ob2_launch; NULL: none) */
   ob2_hlauncher hfn;        /* the loop's halo-folding launcher (set by the
                                stub before ob2_launch; NULL: none) */
+  ob2_tlauncher tfn;        /* the loop's temporal-blocking launcher (2D loops
+                               with one written dat; NULL: none) */
+  const size_t *tb_off;     /* byte offset of each dat argument's view base
+                               in the parameter block (tfn != NULL) */
+  const int *tb_role;       /* per argument: 1 a read dat the chain may
+                               ping-pong, 2 the written dat, 0 other */
 } ob2_loop;
 
 /* A generated launcher: launches one kernel variant with the parameter block
@@ -138,7 +167,9 @@ typedef int (*ob2_mlauncher)(const void *const *params, int n, const unsigned *g
  * the boundary loops of a halo update are the typical case.  A queued halo
  * transfer followed by a run of instances whose loop reads the halos it
  * fills is folded into that run's launch (L->hfn, ob2_hfuse;
- * OPS_B200_HFUSE=0: off).
+ * OPS_B200_HFUSE=0: off).  A run of sweeps at the end of the queue that
+ * ping-pong two dats runs through L->tfn in launches of up to
+ * OPS_B200_TB_DEPTH sweeps (ob2_tblock; OPS_B200_TB=0: off).
  * rows_per_thread: points each thread covers along y (the grid's y extent
  * is derived from it per tile). */
 OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const void *params,

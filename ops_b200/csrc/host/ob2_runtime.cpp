@@ -15,6 +15,9 @@
 // transfers and tridiagonal solves are queued on one CUDA stream and never
 // wait for the device; only reduction results, fetches and host raw pointers
 // synchronise.  Errors surface as OPSException with the reference's codes.
+#include <dlfcn.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -25,6 +28,7 @@
 #include <vector>
 
 #include "ops_b200_device.h"
+#include "ops_b200_dist.h"
 #include "ops_b200_loop.h"
 #include "ops_lib_core.h"
 #include "ops_tridiag.h"
@@ -57,6 +61,16 @@ void tune_decide(KStat &k, int dim);
 
 struct DatX {
   int edat_prev_acc = -1;  // last access kind of an edge dat
+  // slab decomposition (ops_b200_dist.h): the dat holds storage rows
+  // [s_lo, s_hi) of its slowest axis in `alloc`; data_d is offset so that
+  // global storage indices address them
+  bool split = false;
+  char *alloc = nullptr;
+  size_t alloc_bytes = 0, row_bytes = 0;
+  int axis = -1, s_lo = 0, s_hi = 0, H = 0;
+  int o_lo = 0, o_hi = 0;  // owned storage rows
+  bool dirty = false;      // written since its last exchange
+  char *spare = nullptr;   // temporal blocking: second buffer of the dat's storage
 };
 
 struct RedX {
@@ -78,6 +92,13 @@ struct GroupX {
 };
 
 struct Runtime {
+  // slab decomposition over ranks (ops_b200_dist.h); size 1: none
+  ob2_dist_comm comm = {0, 1, 0, nullptr, nullptr, nullptr};
+  bool dist = false;
+  std::vector<std::array<int, 5>> bpart;  // per block: G (-1 unset), lo, hi, first, last
+  char *xstage = nullptr;                 // pinned staging of exchanged rows (host transport)
+  size_t xstage_cap = 0;
+  long long exchanges = 0;
   OPS_instance inst;
   OPS_instance *user = nullptr;  // an application-created instance (C++ API)
   bool initialised = false;
@@ -143,12 +164,22 @@ struct Runtime {
     void *tasks; int ntasks; long long max_pts;  // halo group
     int group;              // halo group index
     ob2_hlauncher hfn;      // halo-folding launcher (NULL: none)
+    ob2_tlauncher tfn;      // temporal-blocking launcher (NULL: none)
+    const size_t *tb_off;   // view-base offsets of the dat arguments in prm
+    const int *tb_role;     // per argument: 1 ping-pong candidate, 2 written dat
+    std::vector<int> acc_arg;  // argument index of each entry of acc
   };
   std::vector<QItem> q;
   struct Graph {
     void *exec = nullptr;
     long long kernels = 0;  // kernel launches the graph replays
     std::string params;     // parameter blocks the graph was captured with
+    // storage swaps of temporal blocking the chain makes (dat, old, new):
+    // repeated on every replay
+    std::vector<std::array<long long, 3>> renames;
+    // the chain's multi-instance, fused, halo-folding and temporal-blocking
+    // launches and sweeps, counted again at every replay
+    long long stats[6] = {0, 0, 0, 0, 0, 0};
   };
   std::unordered_map<std::string, Graph> graph_cache;  // key: the chain's shape
   long long chains = 0, graph_hits = 0, graph_updates = 0, tiles_run = 0, multi_launches = 0;
@@ -158,6 +189,10 @@ struct Runtime {
   long long fused_launches = 0, fused_loops = 0;
   bool hfuse = true;          // fold halo transfers into the consuming launch
   long long hfused = 0;       // halo transfers folded
+  bool tb = true;             // temporal blocking of ping-pong sweep chains
+  int tb_depth = 8;           // sweeps per temporal-blocking launch (OPS_B200_TB_DEPTH)
+  long long tb_launches = 0, tb_sweeps = 0;
+  std::vector<std::array<long long, 3>> *rename_log = nullptr;  // while capturing
 };
 
 Runtime *R = nullptr;
@@ -219,7 +254,10 @@ void ensure_host(ops_dat d) {
 }
 
 /* device -> host when the device copy is newer (ops_lib_core.cpp:2366-2379) */
+void dist_unsupported(ops_dat d, const char *what);
 void get_data(ops_dat d) {
+  if (rt().dist && rt().datx[d->index].split && d->dirty_hd == 2)
+    dist_unsupported(d, "a host copy of the whole dat");
   ensure_host(d);
   ob2_flush();
   if (d->dirty_hd == 2) {
@@ -230,11 +268,169 @@ void get_data(ops_dat d) {
 
 /* host -> device when the host copy is newer (ops_lib_core.cpp:2381-2392) */
 void put_data(ops_dat d) {
+  if (d->dirty_hd == 1 && rt().dist && rt().datx[d->index].split)
+    dist_unsupported(d, "uploading a host copy of the whole dat");
   if (d->dirty_hd == 1) {
     ob2_flush();
     check(ob2_dev_h2d(d->data_d, d->data, d->mem), "ops_put_data");
     d->dirty_hd = 0;
   }
+}
+
+/* ------------------------------------------------------------------------
+ * Slab decomposition over ranks (ops_b200_dist.h).  The partition of a block
+ * is fixed by the first dat declared on it; every dat then holds its owned
+ * storage rows of the slowest axis plus H rows on each inner side.
+ * ---------------------------------------------------------------------- */
+void dist_unsupported(ops_dat d, const char *what) {
+  OPSException ex(OPS_NOT_IMPLEMENTED);
+  ex << "Error: " << what << " (dat " << (d ? d->name : "-")
+     << ") is not supported with the slab decomposition over ranks";
+  throw ex;
+}
+
+std::array<int, 5> &block_part(ops_block b, int G) {
+  Runtime &r = rt();
+  if ((int)r.bpart.size() <= b->index) r.bpart.resize(b->index + 1, {-1, 0, 0, 0, 0});
+  std::array<int, 5> &bp = r.bpart[b->index];
+  if (bp[0] < 0 && G > 0) {
+    bp[0] = G;
+    ob2dist::slab(G, r.comm.size, r.comm.rank, &bp[1], &bp[2]);
+    bp[3] = r.comm.rank == 0;
+    bp[4] = r.comm.rank == r.comm.size - 1;
+    if (bp[2] - bp[1] < 1) {
+      OPSException ex(OPS_INVALID_ARGUMENT);
+      ex << "Error: block " << b->name << " has " << G << " rows along its slowest axis: too "
+         << "few for " << r.comm.size << " ranks";
+      throw ex;
+    }
+  }
+  return bp;
+}
+
+// decides the held rows of a new dat; returns false when it is not split
+bool dist_layout(ops_dat d, DatX &x) {
+  Runtime &r = rt();
+  if (!r.dist) return false;
+  const int ax = d->block->dims - 1;
+  if (ax < 0 || ax > 2 || d->size[ax] == 1) return false;  // edge dats: whole on every rank
+  if (I().OPS_soa && d->dim > 1) dist_unsupported(d, "a multi-component dat in SoA layout");
+  const int n = d->size[ax] + d->d_m[ax] - d->d_p[ax];  // interior extent
+  std::array<int, 5> &bp = block_part(d->block, n);
+  x.split = true;
+  x.axis = ax;
+  x.H = std::max(1, std::max(-d->d_m[ax], d->d_p[ax]));
+  // block rows -> storage rows: s = y - base - d_m
+  const int sh = -d->base[ax] - d->d_m[ax];
+  x.o_lo = bp[3] ? 0 : bp[1] + sh;
+  x.o_hi = bp[4] ? d->size[ax] : std::min(d->size[ax], bp[2] + sh);
+  x.s_lo = bp[3] ? 0 : std::max(0, x.o_lo - x.H);
+  x.s_hi = bp[4] ? d->size[ax] : std::min(d->size[ax], x.o_hi + x.H);
+  if (x.o_hi - x.o_lo < x.H && !(bp[3] && bp[4]))
+    dist_unsupported(d, "a slab thinner than the dat's halo depth");
+  size_t rb = (size_t)d->elem_size;
+  for (int i = 0; i < ax; i++) rb *= (size_t)d->size[i];
+  x.row_bytes = rb;
+  x.alloc_bytes = (size_t)(x.s_hi - x.s_lo) * rb;
+  return true;
+}
+
+void xstage_reserve(size_t n) {
+  Runtime &r = rt();
+  if (n <= r.xstage_cap) return;
+  if (r.xstage) ob2_host_free_pinned(r.xstage);
+  r.xstage = nullptr;
+  check(ob2_host_alloc_pinned((void **)&r.xstage, n), "slab exchange staging");
+  r.xstage_cap = n;
+}
+
+// refreshes the H inner halo rows of a split dat from its neighbours:
+// owned rows [o_lo, o_lo + H) go down into the lower rank's top halo,
+// [o_hi - H, o_hi) up into the upper rank's bottom halo
+void dist_exchange(ops_dat d) {
+  Runtime &r = rt();
+  DatX &x = r.datx[d->index];
+  ob2_flush();
+  const int up = r.comm.rank + 1 < r.comm.size ? r.comm.rank + 1 : -1;
+  const int dn = r.comm.rank > 0 ? r.comm.rank - 1 : -1;
+  const size_t nb = (size_t)x.H * x.row_bytes;
+  char *base = d->data_d;  // global storage row 0
+  char *top_own = base + (size_t)(x.o_hi - x.H) * x.row_bytes;
+  char *top_halo = base + (size_t)x.o_hi * x.row_bytes;
+  char *bot_own = base + (size_t)x.o_lo * x.row_bytes;
+  char *bot_halo = base + (size_t)(x.o_lo - x.H) * x.row_bytes;
+  int e = 0;
+  if (r.comm.device) {  // device buffers, ordered on the work stream
+    e = r.comm.sendrecv(r.comm.ctx, top_own, up >= 0 ? nb : 0, up, bot_halo, dn >= 0 ? nb : 0,
+                        dn);
+    if (!e)
+      e = r.comm.sendrecv(r.comm.ctx, bot_own, dn >= 0 ? nb : 0, dn, top_halo,
+                          up >= 0 ? nb : 0, up);
+  } else {  // host transport: rows staged through pinned memory
+    xstage_reserve(2 * nb);
+    char *sb = r.xstage, *rb = r.xstage + nb;
+    if (up >= 0) check(ob2_dev_d2h(sb, top_own, nb), "slab exchange");
+    e = r.comm.sendrecv(r.comm.ctx, sb, up >= 0 ? nb : 0, up, rb, dn >= 0 ? nb : 0, dn);
+    if (!e && dn >= 0) check(ob2_dev_h2d(bot_halo, rb, nb), "slab exchange");
+    if (!e && dn >= 0) check(ob2_dev_d2h(sb, bot_own, nb), "slab exchange");
+    if (!e) e = r.comm.sendrecv(r.comm.ctx, sb, dn >= 0 ? nb : 0, dn, rb, up >= 0 ? nb : 0, up);
+    if (!e && up >= 0) check(ob2_dev_h2d(top_halo, rb, nb), "slab exchange");
+  }
+  if (e) {
+    OPSException ex(OPS_RUNTIME_ERROR);
+    ex << "Error: slab halo exchange of dat " << d->name << " failed (" << e << ")";
+    throw ex;
+  }
+  x.dirty = false;
+  r.exchanges++;
+}
+
+// before a loop: clips its range along the slowest axis to this rank's rows
+// and refreshes the inner halos of the split dats it reads through a stencil
+// reaching along that axis (when written since their last exchange); marks
+// the split dats it writes as written
+void dist_loop(ops_block block, int dim, int *lo, int *hi, ops_arg *args, int nargs,
+               const char *name) {
+  Runtime &r = rt();
+  if (!r.dist) return;
+  const int ax = dim - 1;
+  if (ax < 0 || ax > 2) return;
+  for (int i = 0; i < nargs; i++) {
+    ops_arg &a = args[i];
+    if (a.argtype != OPS_ARG_DAT || !a.dat || a.acc == OPS_WRITE) continue;
+    DatX &x = r.datx[a.dat->index];
+    if (!x.split) continue;
+    int reach = 0;
+    if (a.stencil) {
+      if (a.stencil->type != 0 || (ax < a.stencil->dims && a.stencil->stride[ax] > 1))
+        dist_unsupported(a.dat, "a strided or multigrid stencil along the split axis");
+      for (int p = 0; p < a.stencil->points; p++)
+        if (ax < a.stencil->dims)
+          reach = std::max(reach, std::abs(a.stencil->stencil[p * a.stencil->dims + ax]));
+    }
+    if (reach > x.H) {
+      OPSException ex(OPS_NOT_IMPLEMENTED);
+      ex << "Error: ops_par_loop " << name << " reads " << a.dat->name << " " << reach
+         << " rows along the split axis, beyond its halo depth " << x.H;
+      throw ex;
+    }
+    if (reach > 0 && x.dirty) dist_exchange(a.dat);
+  }
+  for (int i = 0; i < nargs; i++) {
+    ops_arg &a = args[i];
+    if (a.argtype == OPS_ARG_DAT && a.dat && a.acc != OPS_READ && r.datx[a.dat->index].split)
+      r.datx[a.dat->index].dirty = true;
+  }
+  const std::array<int, 5> &bp = block_part(block, 0);
+  if (bp[0] >= 0) ob2dist::clip(bp[1], bp[2], bp[3], bp[4], &lo[ax], &hi[ax]);
+}
+
+int red_type(const char *t) {
+  if (!strcmp(t, "double")) return 0;
+  if (!strcmp(t, "float")) return 1;
+  if (!strcmp(t, "int")) return 2;
+  if (!strcmp(t, "long long") || !strcmp(t, "ll")) return 3;
+  return -1;
 }
 
 int type_code(const char *t) {
@@ -682,10 +878,178 @@ void run_hfused(std::vector<Runtime::QItem> &q, size_t b, size_t e, const ob2_hf
   kt_end(ev, q[b].kidx);
 }
 
+// ---- temporal blocking of ping-pong sweep chains (ob2_tblock) ----
+// the stencil of an access stays within +-r along x and y (r = 0: the
+// centre only)
+bool tb_stencil_within(const Runtime::QAcc &a, int r) {
+  if (a.any || a.flat || a.mg || a.sidx < 0) return false;
+  const ops_stencil_core *st = rt().stencils[a.sidx];
+  if (st->dims != 2 || st->stride[0] != 1 || st->stride[1] != 1) return false;
+  for (int p = 0; p < st->points; p++)
+    for (int d = 0; d < 2; d++)
+      if (std::abs(st->stencil[2 * p + d]) > r) return false;
+  return true;
+}
+
+// the written dat of an item (entry index in acc), -1: not one
+int tb_written(const Runtime::QItem &it) {
+  int w = -1;
+  for (size_t k = 0; k < it.acc.size(); k++)
+    if (it.acc[k].acc != OPS_READ) {
+      if (w >= 0 || it.acc[k].acc != OPS_WRITE) return -1;
+      w = (int)k;
+    }
+  return w;
+}
+
+bool tb_same_shape(ops_dat a, ops_dat b) {
+  if (a->elem_size != b->elem_size || a->dim != 1 || b->dim != 1) return false;
+  for (int i = 0; i < 2; i++)
+    if (a->size[i] != b->size[i] || a->d_m[i] != b->d_m[i] || a->base[i] != b->base[i])
+      return false;
+  return true;
+}
+
+// items a, b are consecutive sweeps of a ping-pong chain: one loop, a reads
+// dat X through a stencil of reach <= 1 (entry ks) and writes dat Y at the
+// centre (entry kw), b reads Y at entry ks and writes X at entry kw,
+// everything else equal; sets ks and kw
+bool tb_pair(const Runtime::QItem &a, const Runtime::QItem &b, int *ks, int *kw) {
+  Runtime &r = rt();
+  if (a.kind != 0 || b.kind != 0 || !a.tfn || a.tfn != b.tfn || a.fn != b.fn || !a.idx32 ||
+      a.ndim != 2 || a.prm.size() != b.prm.size() || a.acc.size() != b.acc.size() ||
+      a.lo[0] != b.lo[0] || a.hi[0] != b.hi[0] || a.lo[1] != b.lo[1] || a.hi[1] != b.hi[1] ||
+      !a.tb_off || !a.tb_role || r.dist)
+    return false;
+  const int w = tb_written(a);
+  if (w < 0 || tb_written(b) != w) return false;
+  int k = -1;
+  for (size_t e = 0; e < a.acc.size() && k < 0; e++)
+    if ((int)e != w && a.acc[e].acc == OPS_READ && a.acc[e].dat == b.acc[w].dat) k = (int)e;
+  if (k < 0 || b.acc[k].dat != a.acc[w].dat || b.acc[k].acc != OPS_READ) return false;
+  const int argS = a.acc_arg[k], argW = a.acc_arg[w];
+  if (a.tb_role[argS] != 1 || a.tb_role[argW] != 2) return false;
+  if (!tb_stencil_within(a.acc[k], 1) || !tb_stencil_within(a.acc[w], 0) ||
+      !tb_stencil_within(b.acc[k], 1) || !tb_stencil_within(b.acc[w], 0))
+    return false;
+  const int X = a.acc[k].dat, Y = a.acc[w].dat;
+  if (X == Y || !tb_same_shape(r.dats[X], r.dats[Y])) return false;
+  for (size_t e = 0; e < a.acc.size(); e++) {  // every other entry: the same read-only dat
+    if ((int)e == w || (int)e == k) continue;
+    if (a.acc[e].dat != b.acc[e].dat || a.acc[e].acc != OPS_READ || a.acc[e].dat == X ||
+        a.acc[e].dat == Y)
+      return false;
+  }
+  // parameter blocks equal except the two ping-pong view bases
+  const size_t os = a.tb_off[argS], ow = a.tb_off[argW];
+  for (size_t e = 0; e < a.prm.size(); e++)
+    if ((e < os || e >= os + 8) && (e < ow || e >= ow + 8) && a.prm[e] != b.prm[e]) return false;
+  *ks = k;
+  *kw = w;
+  return true;
+}
+
+// end of the ping-pong chain starting at q[i] (i + 1: none); the chain
+// must reach the end of the queue (later items hold the dats' addresses)
+size_t tb_chain(const std::vector<Runtime::QItem> &q, size_t i) {
+  if (!rt().tb || rt().tiling || i + 1 >= q.size()) return i + 1;
+  size_t j = i + 1;
+  int ks, kw;
+  while (j < q.size() && tb_pair(q[j - 1], q[j], &ks, &kw)) j++;
+  if (j != q.size() || j - i < 2) return i + 1;
+  return j;
+}
+
+void tb_spare(ops_dat d) {
+  DatX &x = rt().datx[d->index];
+  if (!x.spare) check(ob2_dev_malloc((void **)&x.spare, d->mem), "temporal blocking");
+}
+
+// allocations before a graph capture (none may happen inside one)
+void tb_prepare(std::vector<Runtime::QItem> &q) {
+  for (size_t i = 0; i < q.size(); i++) {
+    const size_t j = tb_chain(q, i);
+    if (j - i < 2) continue;
+    int ks, kw;
+    if (!tb_pair(q[i], q[i + 1], &ks, &kw)) continue;
+    tb_spare(rt().dats[q[i].acc[ks].dat]);
+    tb_spare(rt().dats[q[i].acc[kw].dat]);
+    i = j - 1;
+  }
+}
+
+void tb_rename(ops_dat d, char *now) {
+  DatX &x = rt().datx[d->index];
+  char *old = d->data_d;
+  d->data_d = now;
+  x.spare = old;
+}
+
+void run_tb(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
+  Runtime &r = rt();
+  size_t a = i;
+  while (a < j) {
+    int ks = -1, kw = -1;
+    // the pair relation of a piece's first sweep with its successor (or,
+    // for the last item, with its predecessor read backwards)
+    if (a + 1 < j) {
+      tb_pair(q[a], q[a + 1], &ks, &kw);
+    } else {
+      run_item(q[a], nullptr, nullptr);  // one sweep left: as it is
+      break;
+    }
+    const size_t b = std::min(j, a + (size_t)r.tb_depth);
+    Runtime::QItem &F = q[a];
+    ops_dat X = r.dats[F.acc[ks].dat];
+    DatX &xx = r.datx[X->index];
+    const int argS = F.acc_arg[ks];
+    char *vs;
+    memcpy(&vs, F.prm.data() + F.tb_off[argS], sizeof vs);
+    ob2_tblock t;
+    memset(&t, 0, sizeof t);
+    t.steps = (int)(b - a);
+    t.s = argS;
+    t.spare = xx.spare + (vs - X->data_d);
+    t.sx0 = X->base[0] + X->d_m[0];
+    t.sx1 = t.sx0 + X->size[0];
+    t.sy0 = X->base[1] + X->d_m[1];
+    t.sy1 = t.sy0 + X->size[1];
+    void *ev = r.capturing ? nullptr : kt_begin();
+    check(F.tfn(F.prm.data(), &t, ob2_dev_stream()), "ops_par_loop launch (temporal blocking)");
+    kt_end(ev, F.kidx);
+    r.launches++;
+    r.tb_launches++;
+    r.tb_sweeps += t.steps;
+    // X's storage is now the spare; later sweeps of the chain address it there
+    char *old = X->data_d, *now = xx.spare;
+    tb_rename(X, now);
+    if (r.rename_log) r.rename_log->push_back({(long long)X->index, (long long)old, (long long)now});
+    for (size_t k = b; k < j; k++) {
+      Runtime::QItem &K = q[k];
+      for (size_t e = 0; e < K.acc.size(); e++) {
+        if (K.acc[e].dat != X->index) continue;
+        char *v;
+        memcpy(&v, K.prm.data() + K.tb_off[K.acc_arg[e]], sizeof v);
+        v = now + (v - old);
+        memcpy(K.prm.data() + K.tb_off[K.acc_arg[e]], &v, sizeof v);
+      }
+    }
+    a = b;
+  }
+}
+
 void run_queue(std::vector<Runtime::QItem> &q) {
   Runtime &r = rt();
   size_t i = 0;
   while (i < q.size()) {
+    if (q[i].kind == 0 && q[i].tfn) {
+      const size_t j = tb_chain(q, i);
+      if (j - i >= 2) {
+        run_tb(q, i, j);
+        i = j;
+        continue;
+      }
+    }
     if (q[i].kind == 1 && i + 1 < q.size() && q[i + 1].kind == 0 && !r.tiling) {
       const size_t j = multi_run(q, i + 1);
       ob2_hfuse h;
@@ -734,6 +1098,7 @@ OPS_API void ob2_flush(void) {
   q.swap(r.q);
   r.chains++;
   if (!r.graphs || r.ktime) {  // per-kernel event timing needs plain launches
+    tb_prepare(q);
     run_queue(q);
     return;
   }
@@ -774,8 +1139,22 @@ OPS_API void ob2_flush(void) {
     r.graph_hits++;
     check(ob2_graph_launch(f->second.exec), "loop-chain graph launch");
     r.launches += f->second.kernels;
+    const long long *st = f->second.stats;
+    r.multi_launches += st[0];
+    r.fused_launches += st[1];
+    r.fused_loops += st[2];
+    r.hfused += st[3];
+    r.tb_launches += st[4];
+    r.tb_sweeps += st[5];
+    for (auto &rn : f->second.renames) {  // the storage swaps the chain makes
+      ops_dat d = r.dats[rn[0]];
+      if (d->data_d != (char *)rn[1])
+        throw OPSException(OPS_RUNTIME_ERROR, "Error: temporal blocking replay out of step");
+      tb_rename(d, (char *)rn[2]);
+    }
     return;
   }
+  tb_prepare(q);
   if (f == r.graph_cache.end() && r.graph_cache.size() >= 256) {
     check(ob2_dev_sync(), "graph cache");
     for (auto &kv : r.graph_cache) ob2_graph_destroy(kv.second.exec);
@@ -785,10 +1164,15 @@ OPS_API void ob2_flush(void) {
   if (G.exec) r.graph_updates++;
   check(ob2_graph_begin_capture(), "loop-chain capture");
   const long long l0 = r.launches;
+  const long long s0[6] = {r.multi_launches, r.fused_launches, r.fused_loops, r.hfused,
+                           r.tb_launches, r.tb_sweeps};
   r.capturing = true;
+  std::vector<std::array<long long, 3>> renames;
+  r.rename_log = &renames;
   try {
     run_queue(q);
   } catch (...) {
+    r.rename_log = nullptr;
     r.capturing = false;
     void *dummy = nullptr;
     ob2_graph_end_capture(&dummy);
@@ -797,12 +1181,17 @@ OPS_API void ob2_flush(void) {
     throw;
   }
   r.capturing = false;
+  r.rename_log = nullptr;
+  G.renames.swap(renames);
   int e = ob2_graph_end_capture(&G.exec);
   if (e) {
     r.graph_cache.erase(shape);
     check(e, "loop-chain capture");
   }
   G.kernels = r.launches - l0;
+  const long long s1[6] = {r.multi_launches, r.fused_launches, r.fused_loops, r.hfused,
+                           r.tb_launches, r.tb_sweeps};
+  for (int k = 0; k < 6; k++) G.stats[k] = s1[k] - s0[k];
   G.params.swap(params);
   check(ob2_graph_launch(G.exec), "loop-chain graph launch");
 }
@@ -863,6 +1252,9 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
   it.max_pts = 0;
   it.group = -1;
   it.hfn = L->hfn;
+  it.tfn = L->tfn;
+  it.tb_off = L->tb_off;
+  it.tb_role = L->tb_role;
   const int td = L->dim - 1;
   for (int i = 0; i < L->nargs; i++) {
     ops_arg &a = L->args[i];
@@ -890,6 +1282,7 @@ OPS_API void ob2_launch(ob2_loop *L, ob2_launcher fn, ob2_mlauncher mfn, const v
     qa.mg = (a.stencil && a.stencil->type != 0) ? 1 : 0;  // restrict / prolong
     if (qa.mg) qa.any = 1;
     it.acc.push_back(qa);
+    it.acc_arg.push_back(i);
   }
   r.q.push_back(std::move(it));
   if (r.max_chain > 0 && (int)r.q.size() >= r.max_chain) ob2_flush();
@@ -915,6 +1308,104 @@ OPS_API void ob2_release_instance(OPS_instance *inst) {
 /* ------------------------------------------------------------------------
  * init / exit  (ops_lib_core.cpp:100-275; ops_cuda_common.cu:68-182)
  * ---------------------------------------------------------------------- */
+/* ------------------------------------------------------------------------
+ * Communicator registration and the runtime's own NCCL transport
+ * (OPS_B200_DIST=nccl: RANK / WORLD_SIZE from the launcher, NCCL loaded at
+ * run time, its unique id passed through a file named after MASTER_ADDR /
+ * MASTER_PORT; rows go GPU to GPU with ncclSend / ncclRecv and reduction
+ * results are combined with ncclAllReduce, all on the work stream).
+ * ---------------------------------------------------------------------- */
+OPS_API int ob2_dist_init(const ob2_dist_comm *c) {
+  Runtime &r = rt();
+  if (!c || c->size < 1 || c->rank < 0 || c->rank >= c->size ||
+      (c->size > 1 && (!c->sendrecv || !c->allreduce)))
+    return OPS_INVALID_ARGUMENT;
+  if (r.initialised && !r.dats.empty()) return OPS_INVALID_ARGUMENT;  // before any dat
+  r.comm = *c;
+  r.dist = c->size > 1;
+  return 0;
+}
+OPS_API int ob2_dist_rank(void) { return rt().comm.rank; }
+OPS_API int ob2_dist_size(void) { return rt().comm.size; }
+
+namespace {
+struct NcclApi {  // the few NCCL entry points used, resolved with dlsym
+  void *h = nullptr;
+  void *comm = nullptr;
+  int (*get_id)(void *id) = nullptr;
+  int (*init_rank)(void **comm, int n, char id[128], int rank) = nullptr;
+  int (*group_start)() = nullptr;
+  int (*group_end)() = nullptr;
+  int (*send)(const void *, size_t, int, int, void *, void *) = nullptr;
+  int (*recv)(void *, size_t, int, int, void *, void *) = nullptr;
+  int (*allreduce)(const void *, void *, size_t, int, int, void *, void *) = nullptr;
+};
+NcclApi g_nccl;
+
+// NCCL's enum values (nccl.h): ncclChar 0, ncclInt32 2, ncclInt64 4,
+// ncclFloat32 7, ncclFloat64 8; ncclSum 0, ncclMax 2, ncclMin 3
+int nccl_sendrecv(void *, const void *sbuf, size_t sb, int sp, void *rbuf, size_t rbn, int rp) {
+  NcclApi &n = g_nccl;
+  void *st = ob2_dev_stream();
+  int e = n.group_start();
+  if (!e && sb && sp >= 0) e = n.send(sbuf, sb, 0, sp, n.comm, st);
+  if (!e && rbn && rp >= 0) e = n.recv(rbuf, rbn, 0, rp, n.comm, st);
+  const int e2 = n.group_end();
+  return e ? e : e2;
+}
+int nccl_allreduce(void *, void *buf, int count, int type, int op) {
+  static const int types[4] = {8, 7, 2, 4};
+  const int o = op == OPS_MAX ? 2 : (op == OPS_MIN ? 3 : 0);
+  if (type < 0 || type > 3) return -1;
+  return g_nccl.allreduce(buf, buf, (size_t)count, types[type], o, g_nccl.comm, ob2_dev_stream());
+}
+
+int nccl_setup() {
+  const char *rk = getenv("RANK"), *ws = getenv("WORLD_SIZE");
+  if (!rk || !ws) return -1;
+  const int rank = atoi(rk), size = atoi(ws);
+  NcclApi &n = g_nccl;
+  n.h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+  if (!n.h) return -2;
+  n.get_id = (int (*)(void *))dlsym(n.h, "ncclGetUniqueId");
+  n.init_rank = (int (*)(void **, int, char *, int))dlsym(n.h, "ncclCommInitRank");
+  n.group_start = (int (*)())dlsym(n.h, "ncclGroupStart");
+  n.group_end = (int (*)())dlsym(n.h, "ncclGroupEnd");
+  n.send = (int (*)(const void *, size_t, int, int, void *, void *))dlsym(n.h, "ncclSend");
+  n.recv = (int (*)(void *, size_t, int, int, void *, void *))dlsym(n.h, "ncclRecv");
+  n.allreduce = (int (*)(const void *, void *, size_t, int, int, void *, void *))dlsym(
+      n.h, "ncclAllReduce");
+  if (!n.get_id || !n.init_rank || !n.group_start || !n.group_end || !n.send || !n.recv ||
+      !n.allreduce)
+    return -3;
+  const char *ma = getenv("MASTER_ADDR"), *mp = getenv("MASTER_PORT");
+  std::string path = std::string("/tmp/ob2_nccl_id_") + (ma ? ma : "local") + "_" + (mp ? mp : "0");
+  char id[128];
+  if (rank == 0) {  // written whole, then renamed into place
+    if (n.get_id(id)) return -4;
+    std::string tmp = path + ".tmp";
+    FILE *f = fopen(tmp.c_str(), "wb");
+    if (!f || fwrite(id, 1, 128, f) != 128) return -5;
+    fclose(f);
+    if (rename(tmp.c_str(), path.c_str())) return -5;
+  } else {  // bounded wait for rank 0's id
+    bool ok = false;
+    for (int t = 0; t < 1200 && !ok; t++) {
+      FILE *f = fopen(path.c_str(), "rb");
+      if (f) {
+        ok = fread(id, 1, 128, f) == 128;
+        fclose(f);
+      }
+      if (!ok) usleep(100000);
+    }
+    if (!ok) return -6;
+  }
+  if (n.init_rank(&n.comm, size, id, rank)) return -7;
+  ob2_dist_comm c = {rank, size, 1, nullptr, nccl_sendrecv, nccl_allreduce};
+  return ob2_dist_init(&c);
+}
+}  // namespace
+
 OPS_API void ops_init(const int argc, const char *const argv[], const int diags) {
   Runtime &r = rt();
   I().OPS_diags = diags;
@@ -949,6 +1440,8 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_MULTI"))) r.multi = atoi(e) != 0;
   if ((e = getenv("OPS_B200_FUSE"))) r.fuse = atoi(e) != 0;
   if ((e = getenv("OPS_B200_HFUSE"))) r.hfuse = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_TB"))) r.tb = atoi(e) != 0;
+  if ((e = getenv("OPS_B200_TB_DEPTH"))) r.tb_depth = std::max(2, std::min(OB2_TB_MAX, atoi(e)));
   if ((e = getenv("OPS_B200_FUSE_PTS"))) r.fuse_pts = atoll(e);
   if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
     r.tune_file = e;
@@ -963,6 +1456,8 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   }
   if (r.cache_mb <= 0.0) r.cache_mb = 40.0;
   if ((e = getenv("OPS_B200_DEVICE"))) r.device = atoi(e);
+  else if ((e = getenv("OPS_B200_DIST")) && !strcmp(e, "nccl") && getenv("LOCAL_RANK"))
+    r.device = atoi(getenv("LOCAL_RANK"));  // one process per GPU
   if ((e = getenv("OPS_B200_BLOCK"))) sscanf(e, "%d,%d,%d", &r.block_x, &r.block_y, &r.block_z);
   if (r.block_x < 1) r.block_x = 32;
   if (r.block_y < 1) r.block_y = 1;
@@ -971,6 +1466,14 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if (I().OPS_diags > 1) r.ktime = true;
   if (r.initialised) return;
   check(ob2_dev_init(r.device), "ops_init (no usable CUDA device)");
+  if ((e = getenv("OPS_B200_DIST")) && !strcmp(e, "nccl") && !r.dist) {
+    const int ne = nccl_setup();  // one process per GPU, rank and size from the launcher
+    if (ne) {
+      OPSException ex(OPS_RUNTIME_ERROR);
+      ex << "Error: OPS_B200_DIST=nccl: NCCL communicator set-up failed (" << ne << ")";
+      throw ex;
+    }
+  }
   check(ob2_dev_sm_count(&r.sms), "ops_init");
   check(ob2_dev_malloc((void **)&r.counter, 4096), "ops_init");
   check(ob2_dev_memset(r.counter, 0, 4096), "ops_init");
@@ -1062,6 +1565,22 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
   d->type = copy_str(type);
   d->name = copy_str(name);
   d->mem = (size_t)d->elem_size * dat_points(d);
+  DatX dxn;
+  d->index = (int)rt().dats.size();
+  if (dist_layout(d, dxn)) {  // this rank's rows only; data_d addresses them globally
+    check(ob2_dev_malloc((void **)&dxn.alloc, dxn.alloc_bytes), "ops_decl_dat (device allocation)");
+    d->data_d = dxn.alloc - (size_t)dxn.s_lo * dxn.row_bytes;
+    if (data) {
+      d->data = data;
+      d->user_managed = 1;
+      check(ob2_dev_h2d(dxn.alloc, data + (size_t)dxn.s_lo * dxn.row_bytes, dxn.alloc_bytes),
+            "ops_decl_dat (upload)");
+    } else {
+      d->data = nullptr;
+      d->user_managed = 0;
+      check(ob2_dev_memset(dxn.alloc, 0, dxn.alloc_bytes), "ops_decl_dat (zero)");
+    }
+  } else {
   check(ob2_dev_malloc((void **)&d->data_d, d->mem), "ops_decl_dat (device allocation)");
   if (data) {
     d->data = data;
@@ -1072,6 +1591,7 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
     d->user_managed = 0;
     check(ob2_dev_memset(d->data_d, 0, d->mem), "ops_decl_dat (zero)");
   }
+  }
   d->dirty_hd = data ? 0 : 2;
   long long off = 0, cum = 1;
   for (int i = 0; i < block->dims; i++) {
@@ -1080,9 +1600,8 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
     cum *= d->size[i];
   }
   d->base_offset = (size_t)off;
-  d->index = (int)rt().dats.size();
   rt().dats.push_back(d);
-  rt().datx.push_back(DatX());
+  rt().datx.push_back(dxn);
   return d;
 }
 
@@ -1092,12 +1611,18 @@ OPS_API void ops_free_dat(ops_dat d) {
   ob2_dev_sync();
   for (auto &p : rt().dats)
     if (p == d) p = nullptr;
-  ob2_dev_free(d->data_d);
+  {
+    DatX &x = rt().datx[d->index];
+    ob2_dev_free(x.split ? x.alloc : d->data_d);
+    if (x.spare) ob2_dev_free(x.spare);
+  }
   if (!d->user_managed) free(d->data);
   free(d);
 }
 
 OPS_API void ops_dat_deep_copy(ops_dat target, ops_dat src) {
+  if (rt().dist && (rt().datx[src->index].split || rt().datx[target->index].split))
+    dist_unsupported(src, "ops_dat_deep_copy");
   require_init();
   ob2_flush();
   if (target->data_d && target->mem != src->mem) {
@@ -1233,11 +1758,31 @@ OPS_API ops_reduction ops_decl_reduction_handle(int size, const char *type, cons
 
 /* ops_lib_core.cpp:1143-1149: forces execution, returns, resets the handle */
 OPS_API void ops_reduction_result_char(ops_reduction h, int, char *ptr) {
-  RedX &x = rt().redx[h->index];
+  Runtime &r = rt();
+  RedX &x = r.redx[h->index];
   if (!x.pending_first) {
     check(ob2_dev_d2h_async(x.host_pinned, x.acc_d, h->size), "ops_reduction_result");
     check(ob2_dev_sync(), "ops_reduction_result");
     memcpy(h->data, x.host_pinned, h->size);
+  } else if (r.dist && h->initialized) {
+    // no point of this rank's rows fed the handle: its part is the identity
+    const int tc = type_code(h->type);
+    const int ts = tc == 1 || tc == 4 || tc == 8 ? 8 : 4;
+    for (int k = 0; k + ts <= h->size; k += ts) identity_bytes(tc, h->acc, h->data + k, false);
+  }
+  if (r.dist) {  // combined over the ranks (the reference's MPI_Allreduce)
+    const int t = red_type(h->type);
+    const int ts = t == 0 || t == 3 ? 8 : 4;
+    if (t < 0) dist_unsupported(nullptr, "a reduction of this type");
+    int e;
+    if (r.comm.device) {
+      check(ob2_dev_h2d(x.acc_d, h->data, h->size), "ops_reduction_result");
+      e = r.comm.allreduce(r.comm.ctx, x.acc_d, h->size / ts, t, h->acc);
+      if (!e) check(ob2_dev_d2h(h->data, x.acc_d, h->size), "ops_reduction_result");
+    } else {
+      e = r.comm.allreduce(r.comm.ctx, h->data, h->size / ts, t, h->acc);
+    }
+    if (e) throw OPSException(OPS_RUNTIME_ERROR, "Error: reduction over the ranks failed");
   }
   memcpy(ptr, h->data, h->size);
   x.pending_first = 0;
@@ -1433,6 +1978,7 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
 
 OPS_API void ops_halo_transfer(ops_halo_group g) {
   require_init();
+  if (rt().dist) dist_unsupported(nullptr, "ops_halo_transfer between blocks");
   GroupX &gx = rt().groupx[g->index];
   bool stale = gx.ntasks != g->nhalos || gx.key.size() != (size_t)2 * g->nhalos;
   for (int hh = 0; !stale && hh < g->nhalos; hh++)
@@ -1465,6 +2011,9 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
     it.max_pts = gx.max_pts;
     it.group = g->index;
     it.hfn = nullptr;
+    it.tfn = nullptr;
+    it.tb_off = nullptr;
+    it.tb_role = nullptr;
     it.ffn = nullptr;
     it.fid = -1;
     it.idx32 = 0;
@@ -1593,6 +2142,19 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   for (int i = 0; i < 3; i++) {
     L->lo[i] = i < dim ? range[2 * i] : 0;
     L->hi[i] = i < dim ? range[2 * i + 1] : 1;
+  }
+  if (r.dist) dist_loop(block, dim, L->lo, L->hi, args, nargs, name);
+  // a loop launched at once (reductions, autotuning) runs the queue first:
+  // a temporally blocked chain in it may move a dat's storage, and the
+  // views below must see where the dats are
+  if (r.autotune || !r.lazy) ob2_flush();
+  else
+    for (int i = 0; i < nargs; i++)
+      if (args[i].argtype == OPS_ARG_GBL && args[i].acc != OPS_READ) {
+        ob2_flush();
+        break;
+      }
+  for (int i = 0; i < 3; i++) {
     L->n[i] = std::max(0, L->hi[i] - L->lo[i]);
     L->npoints *= L->n[i];
   }
@@ -1605,6 +2167,9 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->fuse_id = -1;  // the stub names its fused launcher after this call
   L->ffn = nullptr;
   L->hfn = nullptr;
+  L->tfn = nullptr;
+  L->tb_off = nullptr;
+  L->tb_role = nullptr;
   if (L->npoints == 0) return 0;
 
   size_t red_bytes = 0;
@@ -1846,12 +2411,14 @@ OPS_API long long ob2_launch_count(void) { return rt().launches; }
  * output / timing (ops_lib_core.cpp:1468-1647)
  * ---------------------------------------------------------------------- */
 OPS_API void ops_printf(const char *fmt, ...) {
+  if (R && R->comm.rank != 0) return;  // rank 0 prints, as in the reference's MPI build
   va_list ap;
   va_start(ap, fmt);
   vprintf(fmt, ap);
   va_end(ap);
 }
 OPS_API void ops_fprintf(FILE *f, const char *fmt, ...) {
+  if (R && R->comm.rank != 0) return;
   va_list ap;
   va_start(ap, fmt);
   vfprintf(f, fmt, ap);
@@ -1902,9 +2469,10 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
     snprintf(line, sizeof line,
              "  Lazy execution: %lld chains, %lld graph replays, %lld graph updates, "
              "%lld tile launches, %lld multi-instance launches, %lld fused launches "
-             "(%lld loops), %lld halo transfers folded into loop launches\n",
+             "(%lld loops), %lld halo transfers folded into loop launches, "
+             "%lld temporal-blocking launches (%lld sweeps)\n",
              r.chains, r.graph_hits, r.graph_updates, r.tiles_run, r.multi_launches,
-             r.fused_launches, r.fused_loops, r.hfused);
+             r.fused_launches, r.fused_loops, r.hfused, r.tb_launches, r.tb_sweeps);
     s += line;
   }
   if (buf && n) {
@@ -1933,9 +2501,9 @@ OPS_API void ops_timers(double *cpu, double *et) {
   }
   ops_timers_core(cpu, et);
 }
-OPS_API int ops_is_root(void) { return 1; }
-OPS_API int ops_get_proc(void) { return 0; }
-OPS_API int ops_num_procs(void) { return 1; }
+OPS_API int ops_is_root(void) { return rt().comm.rank == 0; }
+OPS_API int ops_get_proc(void) { return rt().comm.rank; }
+OPS_API int ops_num_procs(void) { return rt().comm.size; }
 OPS_API void ops_NaNcheck(ops_dat d) {
   require_init();
   ops_printf("ops_NaNcheck_core called for %s \n", d->name);
@@ -2041,6 +2609,14 @@ OPS_API void ops_dat_get_extents(ops_dat d, int, int *disp, int *size) {
     if (disp) disp[i] = 0;
     if (size) size[i] = d->size[i] + d->d_m[i] - d->d_p[i];
   }
+  const DatX &x = rt().datx[d->index];
+  if (rt().dist && x.split) {  // this rank's interior rows (as the reference's MPI backend)
+    const int ax = x.axis, sh = -d->d_m[ax];  // storage row of interior row 0
+    const int n = d->size[ax] + d->d_m[ax] - d->d_p[ax];
+    const int a = std::max(0, x.o_lo - sh), b = std::min(n, x.o_hi - sh);
+    if (disp) disp[ax] = a;
+    if (size) size[ax] = std::max(0, b - a);
+  }
 }
 OPS_API size_t ops_dat_get_slab_extents(ops_dat d, int part, int *disp, int *size, int *slab) {
   int ext[OPS_MAX_DIM];
@@ -2071,6 +2647,7 @@ OPS_API void ops_dat_get_raw_metadata(ops_dat d, int part, int *disp, int *size,
 }
 /* ops_dummy_singlenode.cpp:662-707 */
 OPS_API char *ops_dat_get_raw_pointer(ops_dat d, int, ops_stencil, ops_memspace *ms) {
+  if (rt().dist && rt().datx[d->index].split) dist_unsupported(d, "a raw pointer");
   require_init();
   ob2_flush();
   if (ms && *ms == OPS_HOST) {
@@ -2144,11 +2721,11 @@ static void slab_io(ops_dat d, char *data, const int *range, ops_memspace ms, in
   if (dir == 1) d->dirty_hd = 2;
 }
 static void full_range(ops_dat d, int *r) {
-  int ext[OPS_MAX_DIM];
-  ops_dat_get_extents(d, 0, nullptr, ext);
+  int ext[OPS_MAX_DIM], disp[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
+  ops_dat_get_extents(d, 0, disp, ext);
   for (int i = 0; i < OPS_MAX_DIM; i++) {
-    r[2 * i] = 0;
-    r[2 * i + 1] = i < d->block->dims ? ext[i] : 1;
+    r[2 * i] = i < d->block->dims ? disp[i] : 0;
+    r[2 * i + 1] = i < d->block->dims ? disp[i] + ext[i] : 1;
   }
 }
 OPS_API void ops_dat_fetch_data_memspace(ops_dat d, int, char *data, ops_memspace ms) {
@@ -2203,6 +2780,10 @@ OPS_API void ops_fill_random_normal(ops_dat d) { fill_rand(d, 1); }
  * tridiagonal (ops_tridiag_cuda.cpp:96-251: size/type checks, raw pointers
  * at the range origin, solve along solvedim)
  * ---------------------------------------------------------------------- */
+static void trid_dist_check(int ndim, int solvedim, ops_dat d) {
+  if (rt().dist && rt().datx[d->index].split && solvedim == ndim - 1)
+    dist_unsupported(d, "a tridiagonal solve along the split axis");
+}
 static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_dat c, ops_dat d,
                  ops_dat u) {
   require_init();
@@ -2231,6 +2812,15 @@ static void trid(int ndim, int solvedim, int *range, ops_dat a, ops_dat b, ops_d
   int dims[3] = {1, 1, 1};
   long long strides[3] = {1, a->size[0], (long long)a->size[0] * a->size[1]};
   long long off = 0;
+  int rng[6] = {0, 1, 0, 1, 0, 1};
+  for (int i = 0; i < 2 * ndim; i++) rng[i] = range[i];
+  if (rt().dist && rt().datx[d->index].split) {  // lines across the split axis: this rank's
+    trid_dist_check(ndim, solvedim, d);
+    const std::array<int, 5> &bp = block_part(d->block, 0);
+    ob2dist::clip(bp[1], bp[2], bp[3], bp[4], &rng[2 * (ndim - 1)], &rng[2 * ndim - 1]);
+    rt().datx[(u ? u : d)->index].dirty = true;
+  }
+  range = rng;
   for (int i = 0; i < ndim; i++) {
     dims[i] = range[2 * i + 1] - range[2 * i];
     long long s0 = (long long)range[2 * i] - a->d_m[i] - a->base[i];
@@ -2279,10 +2869,39 @@ OPS_API void ops_tridMultiDimBatch_Inc(int ndim, int solvedim, int *range, ops_d
  * dump hook (same format as the oracle): every live dat, halos included
  * ---------------------------------------------------------------------- */
 OPS_API void ops_dump_dats(const char *path) {
-  FILE *f = fopen(path, "wb");
+  Runtime &r = rt();
+  std::string fp(path);
+  if (r.dist) fp += ".r" + std::to_string(r.comm.rank);  // one file per rank
+  FILE *f = fopen(fp.c_str(), "wb");
   if (!f) return;
-  for (ops_dat d : rt().dats) {
+  for (ops_dat d : r.dats) {
     if (!d) continue;
+    const DatX &x = r.datx[d->index];
+    if (r.dist && x.split) {  // this rank's owned storage rows of the slowest axis
+      ob2_flush();
+      const size_t nb = (size_t)(x.o_hi - x.o_lo) * x.row_bytes;
+      std::vector<char> h(nb ? nb : 1);
+      if (nb) check(ob2_dev_d2h(h.data(), d->data_d + (size_t)x.o_lo * x.row_bytes, nb), "dump");
+      int nl = (int)strlen(d->name), tl = (int)strlen(d->type);
+      fwrite("DAT0", 1, 4, f);
+      fwrite(&nl, 4, 1, f);
+      fwrite(d->name, 1, nl, f);
+      fwrite(&tl, 4, 1, f);
+      fwrite(d->type, 1, tl, f);
+      int meta[4] = {d->dim, d->type_size, d->block->dims, I().OPS_soa};
+      fwrite(meta, 4, 4, f);
+      int sz[OPS_MAX_DIM];
+      for (int i = 0; i < OPS_MAX_DIM; i++) sz[i] = d->size[i];
+      sz[x.axis] = x.o_hi - x.o_lo;
+      fwrite(sz, 4, OPS_MAX_DIM, f);
+      fwrite(d->d_m, 4, OPS_MAX_DIM, f);
+      fwrite(d->d_p, 4, OPS_MAX_DIM, f);
+      unsigned long long nbl = nb;
+      fwrite(&nbl, 8, 1, f);
+      fwrite(h.data(), 1, nb, f);
+      continue;
+    }
+    if (r.dist && r.comm.rank != 0) continue;  // whole on every rank: rank 0 writes it
     get_data(d);
     int nl = (int)strlen(d->name);
     fwrite("DAT0", 1, 4, f);

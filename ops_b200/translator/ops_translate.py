@@ -738,6 +738,135 @@ class Translator:
         widest = max([self.ELEM_BYTES.get(p.base_type, 8) for i, a, p in dats] or [8])
         return base * max(1, 8 // widest)
 
+    def tb_candidate(self, loop: Loop, kd):
+        """A 2D loop whose only written argument is one dat (OPS_WRITE, one
+        component), all other dat arguments read-only, no reductions,
+        optional or prolong arguments: its sweeps can be temporally blocked
+        (the runtime checks the stencils and the chain).  Returns (index of
+        the written argument, indices of the read dats of its element type
+        that may be the chain's ping-pong partner) or None."""
+        if loop.ndim != 2:
+            return None
+        ws = []
+        for i, (a, p) in enumerate(zip(loop.args, kd.params)):
+            if a.kind == "reduce" or (a.kind == "dat" and (a.opt or a.prolong)):
+                return None
+            if a.kind == "dat" and a.acc != "OPS_READ":
+                if a.acc != "OPS_WRITE":
+                    return None
+                ws.append(i)
+        if len(ws) != 1:
+            return None
+        wi = ws[0]
+        wt = kd.params[wi].base_type
+        if wt not in ("double", "float") or loop.args[wi].dim.strip() != "1":
+            return None
+        cand = [i for i, (a, p) in enumerate(zip(loop.args, kd.params))
+                if a.kind == "dat" and i != wi and a.acc == "OPS_READ" and p.base_type == wt and
+                a.dim.strip() == "1"]
+        return (wi, cand) if cand else None
+
+    def emit_tblock(self, loop: Loop, kd, P, K, I, dats, tb, w) -> None:
+        """The temporal-blocking kernel of a loop (ob2_tblock in
+        ops_b200_loop.h): CTA tile OB2_TB_TX x OB2_TB_TY of the range, region
+        widened by `steps` in shared memory, the loop's point function on it
+        with the two ping-pong dats' views patched to the shared buffers."""
+        wi, cand = tb
+        T = kd.params[wi].base_type
+        TN = "ob2t_" + loop.stub[len("ops_par_loop_"):]
+        w("template <bool IDX32>")
+        w("__global__ void __launch_bounds__(256) %sT(const __grid_constant__ %s p,"
+          " const __grid_constant__ ob2_tblock t) {" % (K, P))
+        w("  extern __shared__ double ob2_tbsm[];")
+        w("  __shared__ %s pp;  // the parameters with the two dats' views in shared memory" % P)
+        w("  const int S = t.steps, PX = OB2_TB_TX + 2 * S, PY = OB2_TB_TY + 2 * S;")
+        w("  %s *buf0 = (%s *)ob2_tbsm, *buf1 = buf0 + PX * PY;" % (T, T))
+        w("  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;")
+        w("  const int tx0 = p.lo0 + (int)blockIdx.x * OB2_TB_TX, ty0 = p.lo1 + (int)blockIdx.y * OB2_TB_TY;")
+        w("  const int tx1 = min(tx0 + OB2_TB_TX, p.hi0), ty1 = min(ty0 + OB2_TB_TY, p.hi1);")
+        w("  const int X0 = tx0 - S, Y0 = ty0 - S;")
+        # the views of X (arg s) and Y (arg wi): element of (x, y) = b + x*wx + y*wy
+        w("  const %s *gx = nullptr; int xwx = 0, xwy = 0;" % T)
+        for i in cand:
+            w("  if (t.s == %d) { gx = p.b%d; xwx = (int)p.wx%d; xwy = (int)p.wy%d; }" % (i, i, i, i))
+        w("  %s *gy = p.b%d; const int ywx = (int)p.wx%d, ywy = (int)p.wy%d;" % (T, wi, wi, wi))
+        w("  if (tid == 0) {")
+        w("    pp = p;")
+        for i in cand:
+            w("    if (t.s == %d) { pp.wx%d = 1; pp.wy%d = PX; pp.wz%d = 0; pp.ey%d = PX; }" %
+              (i, i, i, i, i))
+        w("    pp.wx%d = 1; pp.wy%d = PX; pp.wz%d = 0; pp.ey%d = PX;" % (wi, wi, wi, wi))
+        w("  }")
+        # load: X over the region within the range widened by one, Y outside
+        # the range (its values there never change)
+        w("  for (int k = tid; k < PX * PY; k += nt) {")
+        w("    const int x = X0 + k % PX, y = Y0 + k / PX;")
+        w("    if (x < p.lo0 - 1 || x > p.hi0 || y < p.lo1 - 1 || y > p.hi1 || x < t.sx0 ||"
+          " x >= t.sx1 || y < t.sy0 || y >= t.sy1) continue;")
+        w("    buf0[k] = gx[x * xwx + y * xwy];")
+        w("    if (x < p.lo0 || x >= p.hi0 || y < p.lo1 || y >= p.hi1) buf1[k] = gy[x * ywx + y * ywy];")
+        w("  }")
+        w("  __syncthreads();")
+        # the sweeps: sweep st reads buffer (st-1)%2 and writes buffer st%2
+        # over the tile widened by S - st, clipped to the range
+        w("  for (int st = 1; st <= S; st++) {")
+        w("    const int m = S - st;")
+        w("    %s *in = (st & 1) ? buf0 : buf1, *out = (st & 1) ? buf1 : buf0;" % T)
+        w("    %s *inv = in - (X0 + Y0 * PX), *outv = out - (X0 + Y0 * PX);" % T)
+        w("    const int rx0 = max(tx0 - m, p.lo0), rx1 = min(tx1 + m, p.hi0);")
+        w("    const int ry0 = max(ty0 - m, p.lo1), ry1 = min(ty1 + m, p.hi1);")
+        w("    const int rw = rx1 - rx0, n = rw > 0 && ry1 > ry0 ? rw * (ry1 - ry0) : 0;")
+        w("    for (int k = tid; k < n; k += nt) {")
+        w("      const int x = rx0 + k % rw, y = ry0 + k / rw;")
+        qs = []
+        for i, a, pr in dats:
+            if i == wi:
+                qs.append("outv")
+            elif i in cand:
+                qs.append("(t.s == %d ? inv : p.b%d)" % (i, i))
+            else:
+                qs.append("p.b%d" % i)
+        w("      %s_A<true>(pp, x, y, 0%s);" % (I, "".join(", " + q for q in qs)))
+        w("    }")
+        w("    __syncthreads();")
+        w("  }")
+        # write back: X's values into its spare, Y's in place; the edge
+        # CTAs also carry X's points outside the range into the spare
+        w("  %s *gs = (%s *)t.spare;" % (T, T))
+        w("  const int ex0 = blockIdx.x == 0 ? t.sx0 : tx0, ex1 = tx1 >= p.hi0 ? t.sx1 : tx1;")
+        w("  const int ey0 = blockIdx.y == 0 ? t.sy0 : ty0, ey1 = ty1 >= p.hi1 ? t.sy1 : ty1;")
+        w("  const int ew = ex1 - ex0, en = ew > 0 && ey1 > ey0 ? ew * (ey1 - ey0) : 0;")
+        w("  for (int k = tid; k < en; k += nt) {")
+        w("    const int x = ex0 + k % ew, y = ey0 + k / ew;")
+        w("    const int gxo = x * xwx + y * xwy;")
+        w("    if (x >= p.lo0 && x < p.hi0 && y >= p.lo1 && y < p.hi1) {")
+        w("      const int b = (x - X0) + (y - Y0) * PX;")
+        w("      gs[gxo] = buf0[b];")
+        w("      gy[x * ywx + y * ywy] = buf1[b];")
+        w("    } else {")
+        w("      gs[gxo] = gx[gxo];")
+        w("    }")
+        w("  }")
+        w("}")
+        w("static int %s(const void *prm, const ob2_tblock *t, void *st) {" % TN)
+        w("  const %s &p = *(const %s *)prm;" % (P, P))
+        w("  if (t->steps < 2 || t->steps > OB2_TB_MAX || !(%s)) return (int)cudaErrorInvalidValue;" %
+          " || ".join("t->s == %d" % i for i in cand))
+        w("  const size_t sm = (size_t)2 * (OB2_TB_TX + 2 * t->steps) * (OB2_TB_TY + 2 * t->steps) *"
+          " sizeof(%s);" % T)
+        w("  static bool attr = false;")
+        w("  if (!attr) {")
+        w("    cudaFuncSetAttribute(%sT<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,"
+          " (int)((size_t)2 * (OB2_TB_TX + 2 * OB2_TB_MAX) * (OB2_TB_TY + 2 * OB2_TB_MAX) *"
+          " sizeof(%s)));" % (K, T))
+        w("    attr = true;")
+        w("  }")
+        w("  const dim3 g((unsigned)((p.hi0 - p.lo0 + OB2_TB_TX - 1) / OB2_TB_TX),"
+          " (unsigned)((p.hi1 - p.lo1 + OB2_TB_TY - 1) / OB2_TB_TY), 1);")
+        w("  %sT<true><<<g, dim3(32, 8, 1), sm, (cudaStream_t)st>>>(p, *t);" % K)
+        w("  return (int)cudaGetLastError();")
+        w("}")
+
     def emit_loop(self, loop: Loop, w) -> None:
         kd = self.kernels[loop.kernel]
         if len(kd.params) != len(loop.args):
@@ -949,6 +1078,9 @@ class Translator:
             w("  __syncthreads();")
             w("  %s<false, IDX32>(p, blockIdx.x, blockIdx.y, bz);" % BF)
             w("}")
+        tb = self.tb_candidate(loop, kd)
+        if tb:
+            self.emit_tblock(loop, kd, P, K, I, dats, tb, w)
         # launchers: the runtime launches a loop now or, in lazy mode, later
         # (possibly once per tile, possibly inside a graph capture)
         LN = "ob2l_" + loop.stub[len("ops_par_loop_"):]
@@ -1059,6 +1191,17 @@ class Translator:
             w("  L.fuse_id = %d;" % len(self.fuse_items))
             w("  L.ffn = ob2f_launch;")
             w("  L.hfn = L.idx32 ? %s_t : %s_f;" % (HN, HN))
+        if tb:
+            TN = "ob2t_" + loop.stub[len("ops_par_loop_"):]
+            offs = ", ".join(("offsetof(%s, b%d)" % (P, i)) if a.kind == "dat" else "0"
+                             for i, a in enumerate(loop.args))
+            roles = ", ".join("2" if i == tb[0] else ("1" if i in tb[1] else "0")
+                              for i in range(len(loop.args)))
+            w("  static const size_t tb_off[%d] = {%s};" % (len(loop.args), offs))
+            w("  static const int tb_role[%d] = {%s};" % (len(loop.args), roles))
+            w("  L.tfn = L.idx32 && !al ? %s : nullptr;" % TN)
+            w("  L.tb_off = tb_off;")
+            w("  L.tb_role = tb_role;")
             self.fuse_items.append((P, "ob2b_" + loop.stub[len("ops_par_loop_"):]))
         w("  ob2_launch(&L, fn, mfn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")

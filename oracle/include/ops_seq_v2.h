@@ -36,6 +36,10 @@ OPS_API void oracle_loop_prologue(const char *name, ops_block block, int dim, co
 OPS_API void oracle_loop_epilogue(const char *name, ops_block block, int dim, const int *range,
                                   ops_arg *args, int nargs);
 OPS_API int oracle_soa(void);
+/* slab decomposition over ranks (ops_b200_dist.h): halo exchanges before the
+ * loop and its range clipped to this rank's rows along the slowest axis */
+OPS_API void oracle_dist_loop(const char *name, ops_block block, int dim, int *lo, int *hi,
+                              ops_arg *args, int nargs);
 
 namespace ops_oracle {
 
@@ -113,6 +117,7 @@ void run(void (*kernel)(P...), std::index_sequence<I...>, const char *name, ops_
     lo[i] = range[2 * i];
     hi[i] = range[2 * i + 1];
   }
+  oracle_dist_loop(name, block, dim, lo, hi, args, N);
   int pt[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
   int gidx[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
   for (int z = lo[2]; z < hi[2]; z++)

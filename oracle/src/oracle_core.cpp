@@ -15,11 +15,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <limits>
 #include <string>
 #include <vector>
 
+#include "ops_b200_dist.h"
 #include "ops_lib_core.h"
 #include "ops_tridiag.h"
 
@@ -32,7 +34,19 @@ struct KernelStat {
   double transfer = 0.0;
 };
 
+struct DistDat {  // the rows a rank holds (see ops_b200_dist.h)
+  bool split = false;
+  char *alloc = nullptr;
+  size_t row_bytes = 0;
+  int axis = -1, s_lo = 0, s_hi = 0, o_lo = 0, o_hi = 0, H = 0;
+  bool dirty = false;
+};
+
 struct OracleState {
+  ob2_dist_comm comm = {0, 1, 0, nullptr, nullptr, nullptr};
+  bool dist = false;
+  std::vector<std::array<int, 5>> bpart;  // per block: G, lo, hi, first, last
+  std::vector<DistDat> dd;
   OPS_instance inst;
   std::vector<ops_block> blocks;
   std::vector<ops_dat> dats;
@@ -99,6 +113,9 @@ template <typename T> void fill_identity(ops_dat d, int acc) {
 OPS_instance *OPS_instance::getOPSInstance() { return &st().inst; }
 
 /* ---- init / exit (ops_lib_core.cpp:267-275; flags :100-249) ---- */
+static bool dist_layout(ops_dat d, DistDat &x);
+static void dist_unsupported(ops_dat d, const char *what);
+
 OPS_API void ops_init(const int argc, const char *const argv[], const int diags) {
   OracleState &s = st();
   s.inst.OPS_diags = diags;
@@ -171,7 +188,14 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
   d->type = copy_str(type);
   d->name = copy_str(name);
   d->mem = (size_t)d->elem_size * dat_points(d);
-  if (data) {
+  DistDat x;
+  if (dist_layout(d, x)) {  // this rank's rows; d->data addresses them by global index
+    x.alloc = (char *)calloc((size_t)(x.s_hi - x.s_lo) * x.row_bytes + 1, 1);
+    if (data)
+      memcpy(x.alloc, data + (size_t)x.s_lo * x.row_bytes, (size_t)(x.s_hi - x.s_lo) * x.row_bytes);
+    d->data = x.alloc - (size_t)x.s_lo * x.row_bytes;
+    d->user_managed = 0;
+  } else if (data) {
     d->data = data;
     d->user_managed = 1;
   } else {
@@ -190,6 +214,7 @@ OPS_API ops_dat ops_decl_dat_char(ops_block block, int dim, int *size, int *base
   d->index = (int)st().dats.size();
   st().dats.push_back(d);
   st().edat_prev_acc.push_back(-1);
+  st().dd.push_back(x);
   return d;
 }
 
@@ -197,7 +222,11 @@ OPS_API void ops_free_dat(ops_dat d) {
   if (!d) return;
   for (auto &p : st().dats)
     if (p == d) p = nullptr;
-  if (!d->user_managed) free(d->data);
+  const DistDat &x = st().dd[d->index];
+  if (x.split)
+    free(x.alloc);
+  else if (!d->user_managed)
+    free(d->data);
   free(d);
 }
 
@@ -234,6 +263,7 @@ OPS_API ops_dat ops_dat_copy(ops_dat src) {
   d->index = (int)st().dats.size();
   st().dats.push_back(d);
   st().edat_prev_acc.push_back(-1);
+  st().dd.push_back(DistDat());
   ops_dat_deep_copy(d, src);
   return d;
 }
@@ -338,6 +368,14 @@ OPS_API ops_reduction ops_decl_reduction_handle(int size, const char *type, cons
 }
 
 OPS_API void ops_reduction_result_char(ops_reduction h, int, char *ptr) {
+  if (st().dist) {  // combined over the ranks (the reference's MPI_Allreduce)
+    int t = !strcmp(h->type, "double") ? 0 : !strcmp(h->type, "float") ? 1
+            : !strcmp(h->type, "int") ? 2 : (!strcmp(h->type, "long long") || !strcmp(h->type, "ll")) ? 3 : -1;
+    if (t < 0) throw OPSException(OPS_NOT_IMPLEMENTED, "Error: reduction type over ranks");
+    const int ts = t == 0 || t == 3 ? 8 : 4;
+    if (st().comm.allreduce(st().comm.ctx, h->data, h->size / ts, t, h->acc))
+      throw OPSException(OPS_RUNTIME_ERROR, "Error: reduction over the ranks failed");
+  }
   memcpy(ptr, h->data, h->size);
   h->initialized = 0;
 }
@@ -413,6 +451,7 @@ OPS_API ops_halo_group ops_decl_halo_group(int nhalos, ops_halo *halos) {
  * bit for bit, converted between float and double when the dat types differ.
  */
 OPS_API void ops_halo_transfer(ops_halo_group g) {
+  if (st().dist) dist_unsupported(nullptr, "ops_halo_transfer between blocks");
   for (int hh = 0; hh < g->nhalos; hh++) {
     ops_halo h = g->halos[hh];
     int n = 1;
@@ -463,6 +502,109 @@ OPS_API void ops_decl_const_char(OPS_instance *, int, char const *, int, char *,
 
 OPS_API void ops_execute(OPS_instance *) {}
 
+/* ---- slab decomposition over ranks (ops_b200_dist.h): the same layout,
+ *      exchanges and clipping as the runtime, on host memory ---- */
+OPS_API int ob2_dist_init(const ob2_dist_comm *c) {
+  if (!c || c->size < 1 || c->rank < 0 || c->rank >= c->size ||
+      (c->size > 1 && (!c->sendrecv || !c->allreduce)) || !st().dats.empty())
+    return OPS_INVALID_ARGUMENT;
+  st().comm = *c;
+  st().dist = c->size > 1;
+  return 0;
+}
+OPS_API int ob2_dist_rank(void) { return st().comm.rank; }
+OPS_API int ob2_dist_size(void) { return st().comm.size; }
+
+static void dist_unsupported(ops_dat d, const char *what) {
+  OPSException ex(OPS_NOT_IMPLEMENTED);
+  ex << "Error: " << what << " (dat " << (d ? d->name : "-")
+     << ") is not supported with the slab decomposition over ranks";
+  throw ex;
+}
+
+static std::array<int, 5> &block_part(ops_block b, int G) {
+  OracleState &o = st();
+  if ((int)o.bpart.size() <= b->index) o.bpart.resize(b->index + 1, {-1, 0, 0, 0, 0});
+  std::array<int, 5> &bp = o.bpart[b->index];
+  if (bp[0] < 0 && G > 0) {
+    bp[0] = G;
+    ob2dist::slab(G, o.comm.size, o.comm.rank, &bp[1], &bp[2]);
+    bp[3] = o.comm.rank == 0;
+    bp[4] = o.comm.rank == o.comm.size - 1;
+    if (bp[2] - bp[1] < 1) throw OPSException(OPS_INVALID_ARGUMENT, "Error: too few rows for the ranks");
+  }
+  return bp;
+}
+
+static bool dist_layout(ops_dat d, DistDat &x) {
+  if (!st().dist) return false;
+  const int ax = d->block->dims - 1;
+  if (ax < 0 || ax > 2 || d->size[ax] == 1) return false;
+  if (st().inst.OPS_soa && d->dim > 1) dist_unsupported(d, "a multi-component dat in SoA layout");
+  const int n = d->size[ax] + d->d_m[ax] - d->d_p[ax];
+  std::array<int, 5> &bp = block_part(d->block, n);
+  x.split = true;
+  x.axis = ax;
+  x.H = std::max(1, std::max(-d->d_m[ax], d->d_p[ax]));
+  const int sh = -d->base[ax] - d->d_m[ax];
+  x.o_lo = bp[3] ? 0 : bp[1] + sh;
+  x.o_hi = bp[4] ? d->size[ax] : std::min(d->size[ax], bp[2] + sh);
+  x.s_lo = bp[3] ? 0 : std::max(0, x.o_lo - x.H);
+  x.s_hi = bp[4] ? d->size[ax] : std::min(d->size[ax], x.o_hi + x.H);
+  if (x.o_hi - x.o_lo < x.H && !(bp[3] && bp[4]))
+    dist_unsupported(d, "a slab thinner than the dat's halo depth");
+  size_t rb = (size_t)d->elem_size;
+  for (int i = 0; i < ax; i++) rb *= (size_t)d->size[i];
+  x.row_bytes = rb;
+  return true;
+}
+
+static void dist_exchange(ops_dat d) {
+  OracleState &o = st();
+  DistDat &x = o.dd[d->index];
+  const int up = o.comm.rank + 1 < o.comm.size ? o.comm.rank + 1 : -1;
+  const int dn = o.comm.rank > 0 ? o.comm.rank - 1 : -1;
+  const size_t nb = (size_t)x.H * x.row_bytes;
+  char *base = d->data;
+  int e = o.comm.sendrecv(o.comm.ctx, base + (size_t)(x.o_hi - x.H) * x.row_bytes, up >= 0 ? nb : 0,
+                          up, base + (size_t)(x.o_lo - x.H) * x.row_bytes, dn >= 0 ? nb : 0, dn);
+  if (!e)
+    e = o.comm.sendrecv(o.comm.ctx, base + (size_t)x.o_lo * x.row_bytes, dn >= 0 ? nb : 0, dn,
+                        base + (size_t)x.o_hi * x.row_bytes, up >= 0 ? nb : 0, up);
+  if (e) throw OPSException(OPS_RUNTIME_ERROR, "Error: slab halo exchange failed");
+  x.dirty = false;
+}
+
+/* exchanges before the loop and clips its slowest-axis range to this rank */
+OPS_API void oracle_dist_loop(const char *name, ops_block block, int dim, int *lo, int *hi,
+                              ops_arg *args, int nargs) {
+  OracleState &o = st();
+  if (!o.dist) return;
+  const int ax = dim - 1;
+  if (ax < 0 || ax > 2) return;
+  for (int i = 0; i < nargs; i++) {
+    ops_arg &a = args[i];
+    if (a.argtype != OPS_ARG_DAT || !a.dat || a.acc == OPS_WRITE) continue;
+    DistDat &x = o.dd[a.dat->index];
+    if (!x.split) continue;
+    int reach = 0;
+    if (a.stencil)
+      for (int p = 0; p < a.stencil->points; p++)
+        if (ax < a.stencil->dims)
+          reach = std::max(reach, std::abs(a.stencil->stencil[p * a.stencil->dims + ax]));
+    if (reach > x.H) dist_unsupported(a.dat, "a stencil deeper than the halo along the split axis");
+    if (reach > 0 && x.dirty) dist_exchange(a.dat);
+  }
+  for (int i = 0; i < nargs; i++) {
+    ops_arg &a = args[i];
+    if (a.argtype == OPS_ARG_DAT && a.dat && a.acc != OPS_READ && o.dd[a.dat->index].split)
+      o.dd[a.dat->index].dirty = true;
+  }
+  const std::array<int, 5> &bp = block_part(block, 0);
+  if (bp[0] >= 0) ob2dist::clip(bp[1], bp[2], bp[3], bp[4], &lo[ax], &hi[ax]);
+  (void)name;
+}
+
 /* ---- par_loop hooks: low-dim accumulation init (ops_dummy_singlenode.cpp:235-391) ---- */
 OPS_API void oracle_loop_prologue(const char *, ops_block, int, const int *, ops_arg *args,
                                   int nargs) {
@@ -511,6 +653,7 @@ OPS_API void oracle_loop_epilogue(const char *name, ops_block block, int, const 
 
 /* ---- output / timing ---- */
 OPS_API void ops_printf(const char *fmt, ...) {
+  if (st().comm.rank != 0) return;  // rank 0 prints
   va_list ap;
   va_start(ap, fmt);
   vprintf(fmt, ap);
@@ -549,9 +692,9 @@ OPS_API void ops_timers_core(double *cpu, double *et) {
   *et = wall();
 }
 OPS_API void ops_timers(double *cpu, double *et) { ops_timers_core(cpu, et); }
-OPS_API int ops_is_root(void) { return 1; }
-OPS_API int ops_get_proc(void) { return 0; }
-OPS_API int ops_num_procs(void) { return 1; }
+OPS_API int ops_is_root(void) { return st().comm.rank == 0; }
+OPS_API int ops_get_proc(void) { return st().comm.rank; }
+OPS_API int ops_num_procs(void) { return st().comm.size; }
 /* ops_dummy_singlenode.cpp:871-878 / ops_lib_core.cpp:1845-1936: the first
  * NaN in (point, component) order stops the program with status 2 */
 OPS_API void ops_NaNcheck(ops_dat d) {
@@ -648,6 +791,14 @@ OPS_API void ops_dat_get_extents(ops_dat d, int, int *disp, int *size) {
     if (disp) disp[i] = 0;
     if (size) size[i] = d->size[i] + d->d_m[i] - d->d_p[i];
   }
+  const DistDat &x = st().dd[d->index];
+  if (st().dist && x.split) {  // this rank's interior rows
+    const int ax = x.axis, sh = -d->d_m[ax];
+    const int n = d->size[ax] + d->d_m[ax] - d->d_p[ax];
+    const int a = std::max(0, x.o_lo - sh), b = std::min(n, x.o_hi - sh);
+    if (disp) disp[ax] = a;
+    if (size) size[ax] = std::max(0, b - a);
+  }
 }
 OPS_API size_t ops_dat_get_slab_extents(ops_dat d, int part, int *disp, int *size, int *slab) {
   int ext[OPS_MAX_DIM];
@@ -672,6 +823,7 @@ OPS_API void ops_dat_get_raw_metadata(ops_dat d, int part, int *disp, int *size,
   }
 }
 OPS_API char *ops_dat_get_raw_pointer(ops_dat d, int, ops_stencil, ops_memspace *ms) {
+  if (st().dist && st().dd[d->index].split) dist_unsupported(d, "a raw pointer");
   if (ms) *ms = OPS_HOST;
   d->locked_hd = 1;
   return d->data + d->base_offset;
@@ -775,10 +927,23 @@ OPS_API void ops_fill_random_normal(ops_dat d) { fill_rand(d, 1); }
 
 /* ---- dump hook shared with the product: every live dat, halos included ---- */
 OPS_API void ops_dump_dats(const char *path) {
-  FILE *f = fopen(path, "wb");
+  std::string fp(path);
+  if (st().dist) fp += ".r" + std::to_string(st().comm.rank);  // one file per rank
+  FILE *f = fopen(fp.c_str(), "wb");
   if (!f) return;
   for (ops_dat d : st().dats) {
     if (!d) continue;
+    const DistDat &x = st().dd[d->index];
+    if (st().dist && !x.split && st().comm.rank != 0) continue;  // rank 0 writes whole dats
+    int sz[OPS_MAX_DIM];
+    for (int i = 0; i < OPS_MAX_DIM; i++) sz[i] = d->size[i];
+    const char *src = d->data;
+    size_t nbytes = d->mem;
+    if (st().dist && x.split) {  // this rank's owned rows
+      sz[x.axis] = x.o_hi - x.o_lo;
+      src = d->data + (size_t)x.o_lo * x.row_bytes;
+      nbytes = (size_t)(x.o_hi - x.o_lo) * x.row_bytes;
+    }
     int nl = (int)strlen(d->name);
     fwrite("DAT0", 1, 4, f);
     fwrite(&nl, 4, 1, f);
@@ -788,12 +953,12 @@ OPS_API void ops_dump_dats(const char *path) {
     fwrite(d->type, 1, tl, f);
     int meta[4] = {d->dim, d->type_size, d->block->dims, st().inst.OPS_soa};
     fwrite(meta, 4, 4, f);
-    fwrite(d->size, 4, OPS_MAX_DIM, f);
+    fwrite(sz, 4, OPS_MAX_DIM, f);
     fwrite(d->d_m, 4, OPS_MAX_DIM, f);
     fwrite(d->d_p, 4, OPS_MAX_DIM, f);
-    unsigned long long nb = d->mem;
+    unsigned long long nb = nbytes;
     fwrite(&nb, 8, 1, f);
-    fwrite(d->data, 1, d->mem, f);
+    fwrite(src, 1, nbytes, f);
   }
   fclose(f);
 }

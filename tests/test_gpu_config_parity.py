@@ -23,6 +23,7 @@ an FP64 value computed in another order); reductions 1e-11 relative.
 
 import json
 import os
+import re
 import subprocess
 import sys
 
@@ -99,6 +100,16 @@ def test_adi_256_matches_oracle(prec, tmp_path):
 
 @pytest.mark.parametrize("prec", ["64", "32"])
 def test_heat_cg_4096_matches_reference_seq(prec, tmp_path):
+    """The dot products are summed in another order than the reference's
+    sequential backend does (a fixed-order tree against a running sum), so
+    alpha and beta move by an ulp and the Krylov vectors r, p, w pick up
+    round-off that the 40 iterations amplify: compared relative to each
+    field's scale (FP64 1e-10, FP32 vectors 1e-4), the FP64 iterate u per
+    element (1e-11) and the mixed form's FP64 iterate x relative to its
+    scale (1e-6); the set-up dats (density, u0, conductivities) exactly; the
+    iteration and replacement counts exactly, the checksums of the solution
+    (reductions) within 1e-11 (FP64) and 1e-6 (mixed)."""
+    import numpy as np
     exe = ensure("heat_cg", "ref_seq", shared=False)
     gd, cd = str(tmp_path / "b200.dump"), str(tmp_path / "ref.dump")
     args = ["-n=4096", "-tol=0", "-maxit=40", "-prec=" + prec]
@@ -108,13 +119,30 @@ def test_heat_cg_4096_matches_reference_seq(prec, tmp_path):
                            timeout=1800)
         assert r.returncode == 0, r.stderr[-2000:]
         cout = r.stdout
-        check(gd, cd)
+        per_elem = compare(gd, cd, mmap=True)
+        scale = compare(gd, cd, mmap=True, floor_frac=1.0)
     finally:
         for p in (gd, cd):
             if os.path.exists(p):
                 os.unlink(p)
+    print("per element", per_elem)
+    print("relative to scale", scale)
+    for name in ("density", "u0", "Kx", "Ky", "Kx32", "Ky32"):
+        if name in per_elem:
+            assert per_elem[name] == 0.0, (name, per_elem[name])
+    if prec == "64":
+        assert per_elem["u"] <= 1e-11, per_elem
+        for name in ("r", "p", "w"):
+            assert scale[name] <= 1e-10, (name, scale[name])
+    else:
+        assert scale["x"] <= 1e-6, scale
+        for name in ("r32", "p32", "w32"):
+            assert scale[name] <= 1e-4, (name, scale[name])
     key = "fp64" if prec == "64" else "mixed"
     g = [l for l in result_lines(gout, (key,)) if "iterations" in l or "checksum" in l]
     c = [l for l in result_lines(cout, (key,)) if "iterations" in l or "checksum" in l]
     assert len(g) == 2, gout[-1000:]
-    assert_lines_close(g, c, 1e-11)
+    words = lambda l: [t for t in l.split() if not re.search(r"[.eE]\d|\d[.eE]", t)]
+    assert [words(l) for l in g] == [words(l) for l in c]
+    ck = lambda lines: [float(l.split()[-1]) for l in lines if "checksum" in l][0]
+    assert abs(ck(g) - ck(c)) <= (1e-11 if prec == "64" else 1e-6) * abs(ck(c))

@@ -76,6 +76,27 @@ def test_halo_transfers_fold_into_the_consuming_launch(args):
     assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
 
 
+@pytest.mark.parametrize("depth,args", [
+    ("2", ["-nb=1", "-n=203", "-sweeps=37", "-check=0"]),
+    ("3", ["-nb=1", "-n=130", "-sweeps=20", "-check=5"]),
+    ("8", ["-nb=1", "-n=257", "-sweeps=45", "-check=0"]),
+    ("8", ["-nb=1", "-n=64", "-sweeps=130", "-check=0"])])
+def test_temporal_blocking_matches_eager(depth, args):
+    """Single-block Jacobi: the queued sweeps ping-pong u and u2, so they run
+    temporally blocked (`depth` sweeps per launch in shared memory, u's
+    storage moving to its spare buffer at every launch); every dat and every
+    printed residual equal eager execution bit for bit (ragged sizes: edge
+    tiles; odd chain lengths: a last sweep on its own; chains longer than 64
+    items: flushes inside the run)."""
+    eo, ed = run_app("poisson_mb", "b200", args, dump=True, env=EAGER)
+    lo, ld = run_app("poisson_mb", "b200", args, dump=True,
+                     env={"OPS_B200_LAZY": "1", "OPS_B200_TB_DEPTH": depth})
+    m = re.search(r"(\d+) temporal-blocking launches \((\d+) sweeps\)", lo)
+    assert m and int(m.group(1)) > 0 and int(m.group(2)) >= int(m.group(1)) * 2, lo[-600:]
+    same(ld, ed)
+    assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
+
+
 @pytest.mark.parametrize("mode", ["lazy_graphs", "tiled_graphs", "tiled_cache"])
 def test_cloverleaf_lazy_matches_eager(tmp_path, mode):
     ensure("clover_step", "b200")
