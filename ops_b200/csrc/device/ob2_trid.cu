@@ -670,16 +670,19 @@ int launch_pipe(const Lines &g, const void *a, const void *b, const void *c, voi
   return (int)cudaGetLastError();
 }
 
-// OB2_TRID_PIPE: 1 (default) solves strided lines of 2 to 256 points with
-// the pipelined persistent kernel, 2 unit-stride lines too, 0 neither.
-// Measured on the 256^3 ADI solves (CUDA events, FP64): y 244 / z 372 us
-// against 258 / 381 us for the line-major CTA kernel, and the FP32-storage
-// step 1.117 against 1.166 ms; unit-stride x lines 451 us against 318 us for
-// the warp-per-line kernel (the chunk-per-lane copies are 8-byte elements
-// 64 bytes apart), so x stays on the latter.  ncu (ADI 256^3, y solve): 24 %
-// of the warp slots active (108-118 registers, 108 KB of shared memory: two
-// CTAs per SM), the stalls split between shared-memory and CTA barriers of
-// the PCR and the FP64 divisions: latency-bound, not memory-bound.
+// OB2_TRID_PIPE: 1 (default) solves strided lines of 2 to 256 points of
+// 4-byte values with the pipelined persistent kernel, 3 strided lines of any
+// value size, 2 unit-stride lines too, 0 none.  Measured on the 256^3 ADI
+// step (CUDA events, 20 steps, two runs each): FP32 storage 0.984-0.985 ms
+// per step pipelined against 1.144-1.149 ms; FP64 1.511-1.512 ms pipelined
+// against 1.410-1.429 ms with the line-major CTA kernel, whose 8-byte rows
+// already keep enough bytes in flight; unit-stride x lines 451 us against
+// 318 us for the warp-per-line kernel (the chunk-per-lane copies are
+// elements 64 bytes apart).  ncu (ADI 256^3, y solve): 24 % of the warp
+// slots active (108-118 registers, 108 KB of shared memory: two CTAs per
+// SM), the stalls split between shared-memory and CTA barriers of the PCR
+// and the FP64 divisions: latency-bound, not memory-bound.
+template <typename T>
 bool use_pipe(const Lines &g) {
   static int v = -1;
   if (v < 0) {
@@ -687,7 +690,8 @@ bool use_pipe(const Lines &g) {
     v = e ? atoi(e) : 1;
   }
   if (g.n < 2 || g.n > 32 * kPipeCL) return false;
-  return g.unit ? v == 2 : v >= 1;
+  if (g.unit) return v == 2;
+  return v >= 2 || (v == 1 && sizeof(T) == 4);
 }
 
 // OB2_TRID_STRIDED: how strided lines are solved.  Measured on the 256^3
@@ -751,7 +755,7 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   g.unit = g.stride == 1 ? 1 : 0;
   if (g.n <= 0 || g.nlines <= 0) return 0;
   if (use_thomas(g.unit)) return launch_thomas<T>(g, a, b, c, d, u);
-  if (use_pipe(g)) {
+  if (use_pipe<T>(g)) {
     if (g.unit) return launch_pipe<T, false>(g, a, b, c, d, u);
     return launch_pipe<T, true>(g, a, b, c, d, u);
   }

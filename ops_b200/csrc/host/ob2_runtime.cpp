@@ -187,9 +187,16 @@ struct Runtime {
   bool fuse = true;           // run independent small loops in one launch
   long long fuse_pts = 65536; // largest loop (points) that is fused
   long long fused_launches = 0, fused_loops = 0;
-  bool hfuse = true;          // fold halo transfers into the consuming launch
+  // fold halo transfers into the consuming launch (OPS_B200_HFUSE=1); off by
+  // default: C1 (2x2 blocks of 256^2) measured 26.5-27.2 GLUPS folded against
+  // 27.3-29.2 unfolded, the CTAs' halo prologue costing more than the launch
+  // it saves
+  bool hfuse = false;
   long long hfused = 0;       // halo transfers folded
-  bool tb = true;             // temporal blocking of ping-pong sweep chains
+  // temporal blocking of ping-pong sweep chains (OPS_B200_TB=1); off by
+  // default: Jacobi 4096^2 (512 sweeps) measured 151 / 203 / 193 GLUPS at
+  // depths 2 / 4 / 8 against 272 GLUPS sweep by sweep
+  bool tb = false;
   int tb_depth = 8;           // sweeps per temporal-blocking launch (OPS_B200_TB_DEPTH)
   long long tb_launches = 0, tb_sweeps = 0;
   std::vector<std::array<long long, 3>> *rename_log = nullptr;  // while capturing

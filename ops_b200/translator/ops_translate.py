@@ -1191,6 +1191,7 @@ class Translator:
             w("  L.fuse_id = %d;" % len(self.fuse_items))
             w("  L.ffn = ob2f_launch;")
             w("  L.hfn = L.idx32 ? %s_t : %s_f;" % (HN, HN))
+            self.fuse_items.append((P, "ob2b_" + loop.stub[len("ops_par_loop_"):]))
         if tb:
             TN = "ob2t_" + loop.stub[len("ops_par_loop_"):]
             offs = ", ".join(("offsetof(%s, b%d)" % (P, i)) if a.kind == "dat" else "0"
@@ -1202,7 +1203,6 @@ class Translator:
             w("  L.tfn = L.idx32 && !al ? %s : nullptr;" % TN)
             w("  L.tb_off = tb_off;")
             w("  L.tb_role = tb_role;")
-            self.fuse_items.append((P, "ob2b_" + loop.stub[len("ops_par_loop_"):]))
         w("  ob2_launch(&L, fn, mfn, &p, sizeof(p), g3, b3, %d);" % (1 if reds else py))
         w("  ob2_loop_end(&L);")
         w("}")

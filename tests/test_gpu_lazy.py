@@ -64,7 +64,8 @@ def test_halo_transfers_fold_into_the_consuming_launch(args):
     cells its stencil reads, then computes); every dat equals eager
     execution bit for bit, and the same with folding switched off."""
     eo, ed = run_app("poisson_mb", "b200", args, dump=True, env=EAGER)
-    lo, ld = run_app("poisson_mb", "b200", args, dump=True, env={"OPS_B200_LAZY": "1"})
+    lo, ld = run_app("poisson_mb", "b200", args, dump=True,
+                     env={"OPS_B200_LAZY": "1", "OPS_B200_HFUSE": "1"})
     no, nd = run_app("poisson_mb", "b200", args, dump=True,
                      env={"OPS_B200_LAZY": "1", "OPS_B200_HFUSE": "0"})
     sweeps = int(args[2].split("=")[1])
@@ -90,7 +91,7 @@ def test_temporal_blocking_matches_eager(depth, args):
     items: flushes inside the run)."""
     eo, ed = run_app("poisson_mb", "b200", args, dump=True, env=EAGER)
     lo, ld = run_app("poisson_mb", "b200", args, dump=True,
-                     env={"OPS_B200_LAZY": "1", "OPS_B200_TB_DEPTH": depth})
+                     env={"OPS_B200_LAZY": "1", "OPS_B200_TB": "1", "OPS_B200_TB_DEPTH": depth})
     m = re.search(r"(\d+) temporal-blocking launches \((\d+) sweeps\)", lo)
     assert m and int(m.group(1)) > 0 and int(m.group(2)) >= int(m.group(1)) * 2, lo[-600:]
     same(ld, ed)

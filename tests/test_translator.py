@@ -144,3 +144,27 @@ def test_cpp_api_constants_and_runtime_length_globals():
     cu = open(os.path.join(out, "c_kernels.cu")).read()
     assert "__constant__ int kc;" in cu
     assert "double g1[64];" in cu and "double g2[NB];" in cu
+
+
+def test_fused_dispatcher_ids_name_each_loops_own_body():
+    """Every stub that offers its loop to the fused dispatcher (ob2fk) names
+    an id whose `case` runs that loop's own body on that loop's parameter
+    block; an id pointing at another loop's body would run it on the wrong
+    parameters."""
+    import re
+    out = tempfile.mkdtemp(prefix="tr_fuse_")
+    src = os.path.join(ROOT, "apps", "opsunit", "opsunit.cpp")
+    Translator([src], [], "opsunit", out).run()
+    cu = open(os.path.join(out, "opsunit_kernels.cu")).read()
+    cases = {int(k): (body, prm) for k, body, prm in
+             re.findall(r"case (\d+): (ob2b_\w+)<false, IDX32>\(\*\(const (\w+) \*\)prm", cu)}
+    stubs = re.findall(r"void (ops_par_loop_\w+)\(.*?\n\}\n", cu, flags=re.S)
+    ids = {}
+    for m in re.finditer(r"void ops_par_loop_(\w+)\((.*?)\n\}\n", cu, flags=re.S):
+        f = re.search(r"L\.fuse_id = (\d+);", m.group(2))
+        if f:
+            ids[m.group(1)] = int(f.group(1))
+    assert stubs and ids and len(set(ids.values())) == len(ids)
+    for name, k in ids.items():
+        assert k in cases, (name, k)
+        assert cases[k][0] == "ob2b_" + name and cases[k][1].startswith("ob2p_"), (name, cases[k])
