@@ -16,12 +16,18 @@
 //   * each thread substitutes its chunk and writes the solution (or adds it
 //     to u for the _Inc form, leaving d untouched).
 //
-// Lines of up to 32*CL points use one warp per line and PCR with warp
-// shuffles (no shared memory, no CTA barriers).  For strided lines (y, z)
-// the CTA's 8 lines are staged through shared memory so that loads and
-// stores are contiguous runs along x (or, on request, one thread per line
-// runs the Thomas algorithm: trid_thomas_kernel).  Longer lines use a CTA per
-// group of lines with PCR in shared memory.  Each coefficient is read once and the
+// Lines of up to 256 points: unit-stride lines (x) one warp per line with
+// vector loads and stores of each lane's 8-point chunk (trid_xw_kernel);
+// strided lines (y, z) 8 neighbouring lines per CTA, consecutive threads on
+// the same chunk of neighbouring lines so that every warp access is
+// contiguous runs along x, each line's PCR in one warp after one exchange
+// through shared memory (trid_lmw_kernel).  The reciprocals of the
+// eliminations come from a Newton-Raphson refinement of the hardware
+// approximation (rcp64).  Other forms stay selectable (OB2_TRID_*): a
+// scalar warp-per-line kernel, a staged one, line-major CTA kernels with
+// the PCR in shared memory, a pipelined persistent one, and the Thomas
+// algorithm one thread per line (trid_thomas_kernel).  Longer lines use a
+// CTA per group of lines with PCR in shared memory.  Each coefficient is read once and the
 // solution written once: the DRAM traffic is the algorithmic 5 values per
 // point (7 for _Inc).  Elimination is FP64 for double and float storage.
 // Every register array is indexed with compile-time indices only (a run-time
@@ -38,6 +44,24 @@ namespace {
 
 constexpr int kThreads = 256;  // CTA size
 
+// 1 / x for the eliminations: the Newton-Raphson iteration
+// y <- y + y (1 - x y), each step doubling the correct bits, twice from the
+// hardware reciprocal approximation (PTX rcp.approx.ftz.f64), with fused
+// multiply-adds; zeros, infinities, NaNs and magnitudes whose reciprocal
+// could leave the normal range take the IEEE division.  On the GPU the
+// result equals 1.0 / x in every bit over 4M random inputs with exponents in
+// [-60, 60]; it replaces a division sequence that is several times longer.
+__device__ __forceinline__ double rcp64(double x) {
+  const double ax = fabs(x);
+  if (!(ax > 0x1p-1000 && ax < 0x1p1000)) return 1.0 / x;
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = __fma_rn(-x, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-x, y, 1.0);
+  return __fma_rn(y, e, y);
+}
+
 // After chunk_reduce (all CL rows; padding rows are b = 1, a = c = d = 0),
 // row i of the chunk reads
 //   a_i * x_first + x_i + c_i * x_last = d_i        (0 < i < CL-1)
@@ -47,15 +71,15 @@ constexpr int kThreads = 256;  // CTA size
 template <int CL>
 __device__ __forceinline__ void chunk_reduce(double *a, const double *b, double *c, double *d) {
   {
-    double r = 1.0 / b[0];
+    double r = rcp64(b[0]);
     a[0] *= r; c[0] *= r; d[0] *= r;
-    r = 1.0 / b[1];
+    r = rcp64(b[1]);
     a[1] *= r; c[1] *= r; d[1] *= r;
   }
   // forward: row i (i >= 2) loses x_{i-1}, gains x_0
 #pragma unroll
   for (int i = 2; i < CL; i++) {
-    const double r = 1.0 / (b[i] - a[i] * c[i - 1]);
+    const double r = rcp64(b[i] - a[i] * c[i - 1]);
     d[i] = r * (d[i] - a[i] * d[i - 1]);
     a[i] = -r * a[i] * a[i - 1];
     c[i] = r * c[i];
@@ -69,7 +93,7 @@ __device__ __forceinline__ void chunk_reduce(double *a, const double *b, double 
   }
   // row 0 loses x_1, gains x_{CL-1}
   {
-    const double r = 1.0 / (1.0 - c[0] * a[1]);
+    const double r = rcp64(1.0 - c[0] * a[1]);
     d[0] = r * (d[0] - c[0] * d[1]);
     a[0] = r * a[0];
     c[0] = -r * c[0] * c[1];
@@ -91,12 +115,12 @@ __device__ __forceinline__ void warp_pcr(double a0, double c0, double d0, double
                  nd0 = __shfl_down_sync(full, d0, 1);
     const bool hasl = lane > 0, hasr = lane < 31;
     double k1 = hasl ? a0 : 0.0, k2 = c0;
-    double inv = 1.0 / (1.0 - k1 * (hasl ? pc1 : 0.0) - k2 * a1);
+    double inv = rcp64(1.0 - k1 * (hasl ? pc1 : 0.0) - k2 * a1);
     const double A0 = -k1 * (hasl ? pa1 : 0.0) * inv, C0 = -k2 * c1 * inv,
                  D0 = (d0 - k1 * (hasl ? pd1 : 0.0) - k2 * d1) * inv;
     k1 = a1;
     k2 = hasr ? c1 : 0.0;
-    inv = 1.0 / (1.0 - k1 * c0 - k2 * (hasr ? na0 : 0.0));
+    inv = rcp64(1.0 - k1 * c0 - k2 * (hasr ? na0 : 0.0));
     const double A1 = -k1 * a0 * inv, C1 = -k2 * (hasr ? nc0 : 0.0) * inv,
                  D1 = (d1 - k1 * d0 - k2 * (hasr ? nd0 : 0.0)) * inv;
     a0 = A0; c0 = C0; d0 = D0;
@@ -116,14 +140,14 @@ __device__ __forceinline__ void warp_pcr(double a0, double c0, double d0, double
                  rd1 = __shfl_down_sync(full, d1, h);
     {
       const double k1 = hasl ? a0 : 0.0, k2 = hasr ? c0 : 0.0;
-      const double inv = 1.0 / (1.0 - k1 * (hasl ? lc0 : 0.0) - k2 * (hasr ? ra0 : 0.0));
+      const double inv = rcp64(1.0 - k1 * (hasl ? lc0 : 0.0) - k2 * (hasr ? ra0 : 0.0));
       const double nA = -k1 * (hasl ? la0 : 0.0) * inv, nC = -k2 * (hasr ? rc0 : 0.0) * inv;
       d0 = (d0 - k1 * (hasl ? ld0 : 0.0) - k2 * (hasr ? rd0 : 0.0)) * inv;
       a0 = nA; c0 = nC;
     }
     {
       const double k1 = hasl ? a1 : 0.0, k2 = hasr ? c1 : 0.0;
-      const double inv = 1.0 / (1.0 - k1 * (hasl ? lc1 : 0.0) - k2 * (hasr ? ra1 : 0.0));
+      const double inv = rcp64(1.0 - k1 * (hasl ? lc1 : 0.0) - k2 * (hasr ? ra1 : 0.0));
       const double nA = -k1 * (hasl ? la1 : 0.0) * inv, nC = -k2 * (hasr ? rc1 : 0.0) * inv;
       d1 = (d1 - k1 * (hasl ? ld1 : 0.0) - k2 * (hasr ? rd1 : 0.0)) * inv;
       a1 = nA; c1 = nC;
@@ -171,6 +195,146 @@ __global__ void __launch_bounds__(kThreads) trid_warp_kernel(
       else
         D[e] = (T)x;
     }
+}
+
+// Eight consecutive elements from p into FP64 registers with the widest
+// aligned vector loads (16 bytes when p allows; p's alignment is uniform
+// over a warp whose lanes start chunks of 8 elements of one line).
+template <typename T>
+__device__ __forceinline__ void load8(const T *p, double (&v)[8]) {
+  const uintptr_t ad = (uintptr_t)p;
+  if (sizeof(T) == 8) {
+    const double *q = (const double *)p;
+    if ((ad & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const double2 t = ((const double2 *)q)[i];
+        v[2 * i] = t.x; v[2 * i + 1] = t.y;
+      }
+    } else {
+      v[0] = q[0];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const double2 t = ((const double2 *)(q + 1))[i];
+        v[2 * i + 1] = t.x; v[2 * i + 2] = t.y;
+      }
+      v[7] = q[7];
+    }
+  } else {
+    const float *q = (const float *)p;
+    if ((ad & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const float4 t = ((const float4 *)q)[i];
+        v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+      }
+    } else if ((ad & 7) == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float2 t = ((const float2 *)q)[i];
+        v[2 * i] = t.x; v[2 * i + 1] = t.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) v[i] = q[i];
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store8(T *p, const double (&v)[8]) {
+  const uintptr_t ad = (uintptr_t)p;
+  if (sizeof(T) == 8) {
+    double *q = (double *)p;
+    if ((ad & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) ((double2 *)q)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    } else {
+      q[0] = v[0];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        ((double2 *)(q + 1))[i] = make_double2(v[2 * i + 1], v[2 * i + 2]);
+      q[7] = v[7];
+    }
+  } else {
+    float *q = (float *)p;
+    if ((ad & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+        ((float4 *)q)[i] = make_float4((float)v[4 * i], (float)v[4 * i + 1], (float)v[4 * i + 2],
+                                       (float)v[4 * i + 3]);
+    } else if ((ad & 7) == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) ((float2 *)q)[i] = make_float2((float)v[2 * i], (float)v[2 * i + 1]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) q[i] = (float)v[i];
+    }
+  }
+}
+
+// Unit-stride lines of up to 256 points, one warp per line, 8-point chunks
+// per lane: a lane whose chunk lies inside the line loads and stores it
+// with 16-byte vector accesses (8-byte ones and single elements where the
+// line's alignment leaves no choice), the line's last, partial chunk element
+// by element.  32-bit element offsets when every offset of the batch fits
+// (IDX32).  Three CTAs per SM.
+template <typename T, bool INC, bool IDX32>
+__global__ void __launch_bounds__(kThreads, 3) trid_xw_kernel(
+    int n, long long nlines, int o1n, long long o1s, long long o2s, const T *__restrict__ A,
+    const T *__restrict__ B, const T *__restrict__ C, T *__restrict__ D, T *__restrict__ U) {
+  constexpr int CL = 8;
+  const int lane = threadIdx.x & 31;
+  const long long line = (long long)blockIdx.x * (kThreads >> 5) + (threadIdx.x >> 5);
+  if (line >= nlines) return;  // the whole warp leaves together
+  const int k0 = lane * CL;
+  const long long base =
+      IDX32 ? (long long)((int)(line % o1n) * (int)o1s + (int)(line / o1n) * (int)o2s + k0)
+            : (line % o1n) * o1s + (line / o1n) * o2s + k0;
+  const int len = max(0, min(CL, n - k0));
+  double a[CL], b[CL], c[CL], d[CL];
+  if (len == CL) {
+    load8(A + base, a);
+    load8(B + base, b);
+    load8(C + base, c);
+    load8(D + base, d);
+  } else {
+#pragma unroll
+    for (int i = 0; i < CL; i++) {
+      a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
+      if (i < len) {
+        a[i] = (double)A[base + i];
+        b[i] = (double)B[base + i];
+        c[i] = (double)C[base + i];
+        d[i] = (double)D[base + i];
+      }
+    }
+  }
+  if (k0 == 0) a[0] = 0.0;  // no left neighbour
+#pragma unroll
+  for (int i = 0; i < CL; i++)
+    if (k0 + i == n - 1) c[i] = 0.0;  // no right neighbour
+  chunk_reduce<CL>(a, b, c, d);
+  double xf, xl;
+  warp_pcr(a[0], c[0], d[0], a[CL - 1], c[CL - 1], d[CL - 1], lane, xf, xl);
+  double x[CL];
+#pragma unroll
+  for (int i = 0; i < CL; i++)
+    x[i] = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+  T *out = (INC ? U : D) + base;
+  if (len == CL) {
+    if (INC) {
+      double u[CL];
+      load8(out, u);
+#pragma unroll
+      for (int i = 0; i < CL; i++) x[i] += u[i];
+    }
+    store8(out, x);
+  } else {
+#pragma unroll
+    for (int i = 0; i < CL; i++)
+      if (i < len) out[i] = INC ? (T)((double)out[i] + x[i]) : (T)x[i];
+  }
 }
 
 // Staged warp-per-line form: the CTA's W = 8 lines pass through shared memory
@@ -303,7 +467,7 @@ __global__ void __launch_bounds__(kThreads) trid_cta_kernel(
       if (hl) { a1 = ra[r - s]; c1 = rc[r - s]; d1 = rd[r - s]; }
       if (hr) { a2 = ra[r + s]; c2 = rc[r + s]; d2 = rd[r + s]; }
       const double k1l = hl ? ar : 0.0, k2r = hr ? cr : 0.0;
-      const double inv = 1.0 / (1.0 - k1l * c1 - k2r * a2);
+      const double inv = rcp64(1.0 - k1l * c1 - k2r * a2);
       na[q] = -k1l * a1 * inv;
       nc[q] = -k2r * c2 * inv;
       nd[q] = (dr - k1l * d1 - k2r * d2) * inv;
@@ -322,6 +486,74 @@ __global__ void __launch_bounds__(kThreads) trid_cta_kernel(
     if (i < len) {
       const double x = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
       const long long e = base + (long long)(k0 + i) * stride;
+      if (INC)
+        U[e] = (T)((double)U[e] + x);
+      else
+        D[e] = (T)x;
+    }
+}
+
+// Strided lines of up to 256 points (y, z): 8 lines x 32 chunks of 8 points
+// per CTA in the line-major mapping of trid_cta_kernel (consecutive threads
+// on the same chunk of neighbouring lines, whose elements are contiguous:
+// every load and store of a warp is runs of 8 elements), but the PCR over
+// each line's 64 chunk-end unknowns runs in one warp with shuffles (warp w
+// solves line w): the end rows cross shared memory once each way, with two
+// CTA barriers instead of two per PCR level.  Three CTAs per SM; 32-bit
+// element offsets when every offset of the batch fits (IDX32).
+template <typename T, bool INC, bool IDX32>
+__global__ void __launch_bounds__(kThreads, 3) trid_lmw_kernel(
+    int n, long long nlines, long long stride, int o1n, long long o1s, long long o2s,
+    const T *__restrict__ A, const T *__restrict__ B, const T *__restrict__ C,
+    T *__restrict__ D, T *__restrict__ U) {
+  constexpr int CL = 8, P = 32, LPB = kThreads / P, M = 2 * P, pitch = 3 * M + 1;
+  static_assert(LPB == kThreads / 32, "one warp per line for the PCR");
+  __shared__ double sm[LPB * pitch];
+  const int tid = threadIdx.x;
+  const int p = tid / LPB, l = tid % LPB;
+  const long long line = (long long)blockIdx.x * LPB + l;
+  const bool active = line < nlines;
+  const int k0 = p * CL;
+  long long base = 0;
+  if (active)
+    base = IDX32 ? (long long)((int)(line % o1n) * (int)o1s + (int)(line / o1n) * (int)o2s +
+                               k0 * (int)stride)
+                 : (line % o1n) * o1s + (line / o1n) * o2s + (long long)k0 * stride;
+  const int len = active ? max(0, min(CL, n - k0)) : 0;
+  double a[CL], b[CL], c[CL], d[CL];
+#pragma unroll
+  for (int i = 0; i < CL; i++) {
+    a[i] = 0.0; b[i] = 1.0; c[i] = 0.0; d[i] = 0.0;
+    if (i < len) {
+      const long long e = IDX32 ? (long long)((int)base + i * (int)stride) : base + i * stride;
+      a[i] = (k0 + i == 0) ? 0.0 : (double)A[e];
+      b[i] = (double)B[e];
+      c[i] = (k0 + i == n - 1) ? 0.0 : (double)C[e];
+      d[i] = (double)D[e];
+    }
+  }
+  chunk_reduce<CL>(a, b, c, d);
+  double *ra = sm + l * pitch, *rc = ra + M, *rd = rc + M;
+  ra[2 * p] = a[0]; rc[2 * p] = c[0]; rd[2 * p] = d[0];
+  ra[2 * p + 1] = a[CL - 1]; rc[2 * p + 1] = c[CL - 1]; rd[2 * p + 1] = d[CL - 1];
+  __syncthreads();
+  {
+    const int w = tid >> 5, lane = tid & 31;
+    double *wa = sm + w * pitch, *wc = wa + M, *wd = wc + M;
+    double xf, xl;
+    warp_pcr(wa[2 * lane], wc[2 * lane], wd[2 * lane], wa[2 * lane + 1], wc[2 * lane + 1],
+             wd[2 * lane + 1], lane, xf, xl);
+    wd[2 * lane] = xf;  // this lane's own rows: no other lane reads them
+    wd[2 * lane + 1] = xl;
+  }
+  __syncthreads();
+  if (len <= 0) return;
+  const double xf = rd[2 * p], xl = rd[2 * p + 1];
+#pragma unroll
+  for (int i = 0; i < CL; i++)
+    if (i < len) {
+      const double x = (i == 0) ? xf : ((i == CL - 1) ? xl : d[i] - a[i] * xf - c[i] * xl);
+      const long long e = IDX32 ? (long long)((int)base + i * (int)stride) : base + i * stride;
       if (INC)
         U[e] = (T)((double)U[e] + x);
       else
@@ -444,7 +676,7 @@ __global__ void __launch_bounds__(kThreads, 2) trid_pipe_kernel(
         if (hl) { a1 = ra[r - s]; c1 = rc[r - s]; d1 = rd[r - s]; }
         if (hr) { a2 = ra[r + s]; c2 = rc[r + s]; d2 = rd[r + s]; }
         const double k1l = hl ? ar : 0.0, k2r = hr ? cr : 0.0;
-        const double inv = 1.0 / (1.0 - k1l * c1 - k2r * a2);
+        const double inv = rcp64(1.0 - k1l * c1 - k2r * a2);
         na[q] = -k1l * a1 * inv;
         nc[q] = -k2r * c2 * inv;
         nd[q] = (dr - k1l * d1 - k2r * d2) * inv;
@@ -595,6 +827,60 @@ int launch_warp(const Lines &g, const void *a, const void *b, const void *c, voi
   return (int)cudaGetLastError();
 }
 
+// 1: every element offset of the batch fits 32-bit arithmetic
+bool offsets_fit32(const Lines &g) {
+  if (g.o1s < 0 || g.o2s < 0 || g.stride < 0) return false;
+  const long long d2 = (g.nlines + g.o1n - 1) / g.o1n;
+  const long long mx =
+      (long long)(g.o1n - 1) * g.o1s + (d2 - 1) * g.o2s + (long long)(g.n - 1) * g.stride;
+  return mx < 0x7fffffffLL;
+}
+
+template <typename T>
+int launch_xw(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  const long long grid = (g.nlines + (kThreads / 32) - 1) / (kThreads / 32);
+  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  const bool i32 = offsets_fit32(g);
+  const T *A = (const T *)a, *B = (const T *)b, *C = (const T *)c;
+  T *D = (T *)d, *U = (T *)u;
+  if (u) {
+    if (i32)
+      trid_xw_kernel<T, true, true><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.o1n, g.o1s, g.o2s, A, B, C, D, U);
+    else
+      trid_xw_kernel<T, true, false><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.o1n, g.o1s, g.o2s, A, B, C, D, U);
+  } else {
+    if (i32)
+      trid_xw_kernel<T, false, true><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.o1n, g.o1s, g.o2s, A, B, C, D, nullptr);
+    else
+      trid_xw_kernel<T, false, false><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.o1n, g.o1s, g.o2s, A, B, C, D, nullptr);
+  }
+  return (int)cudaGetLastError();
+}
+
+template <typename T>
+int launch_lmw(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
+  constexpr int LPB = kThreads / 32;
+  const long long grid = (g.nlines + LPB - 1) / LPB;
+  if (grid > 0x7fffffffLL) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = (cudaStream_t)ob2_dev_stream();
+  const bool i32 = offsets_fit32(g);
+  const T *A = (const T *)a, *B = (const T *)b, *C = (const T *)c;
+  T *D = (T *)d, *U = (T *)u;
+  if (u) {
+    if (i32)
+      trid_lmw_kernel<T, true, true><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, A, B, C, D, U);
+    else
+      trid_lmw_kernel<T, true, false><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, A, B, C, D, U);
+  } else {
+    if (i32)
+      trid_lmw_kernel<T, false, true><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, A, B, C, D, nullptr);
+    else
+      trid_lmw_kernel<T, false, false><<<(unsigned)grid, kThreads, 0, st>>>(g.n, g.nlines, g.stride, g.o1n, g.o1s, g.o2s, A, B, C, D, nullptr);
+  }
+  return (int)cudaGetLastError();
+}
+
 template <typename T, int CL>
 int launch_staged(const Lines &g, const void *a, const void *b, const void *c, void *d, void *u) {
   const int W = kThreads / 32;
@@ -670,15 +956,14 @@ int launch_pipe(const Lines &g, const void *a, const void *b, const void *c, voi
   return (int)cudaGetLastError();
 }
 
-// OB2_TRID_PIPE: 1 (default) solves strided lines of 2 to 256 points of
-// 4-byte values with the pipelined persistent kernel, 3 strided lines of any
-// value size, 2 unit-stride lines too, 0 none.  Measured on the 256^3 ADI
-// step (CUDA events, 20 steps, two runs each): FP32 storage 0.984-0.985 ms
-// per step pipelined against 1.144-1.149 ms; FP64 1.511-1.512 ms pipelined
-// against 1.410-1.429 ms with the line-major CTA kernel, whose 8-byte rows
-// already keep enough bytes in flight; unit-stride x lines 451 us against
-// 318 us for the warp-per-line kernel (the chunk-per-lane copies are
-// elements 64 bytes apart).  ncu (ADI 256^3, y solve): 24 % of the warp
+// OB2_TRID_PIPE: 0 (default) none, 1 strided lines of 2 to 256 points of
+// 4-byte values through the pipelined persistent kernel, 3 strided lines of
+// any value size, 2 unit-stride lines too.  Measured on the 256^3 ADI lines
+// (CUDA events): FP32 y / z 225 / 307 us pipelined against 173 / 279 us
+// for trid_lmw_kernel; FP64 step 1.511-1.512 ms pipelined against
+// 1.410-1.429 ms with the line-major CTA kernel; unit-stride x lines 451 us
+// against 318 us for the warp-per-line kernel (the chunk-per-lane copies
+// are elements 64 bytes apart).  ncu (ADI 256^3, y solve): 24 % of the warp
 // slots active (108-118 registers, 108 KB of shared memory: two CTAs per
 // SM), the stalls split between shared-memory and CTA barriers of the PCR
 // and the FP64 divisions: latency-bound, not memory-bound.
@@ -687,7 +972,7 @@ bool use_pipe(const Lines &g) {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("OB2_TRID_PIPE");
-    v = e ? atoi(e) : 1;
+    v = e ? atoi(e) : 0;
   }
   if (g.n < 2 || g.n > 32 * kPipeCL) return false;
   if (g.unit) return v == 2;
@@ -695,15 +980,18 @@ bool use_pipe(const Lines &g) {
 }
 
 // OB2_TRID_STRIDED: how strided lines are solved.  Measured on the 256^3
-// FP64 y / z solves (CUDA events, 20 steps): 3 the line-major CTA kernel
-// with 8-point chunks (8 lines x 32 chunks per CTA, 64-byte runs, 2 CTAs per
-// SM): 226 / 364 us; 2 the same with 16-point chunks (16 lines, 128-byte
-// runs, 150 registers, 1 CTA per SM): 213 / 438 us; 1 the staged
-// warp-per-line kernel: 300 / 408 us; 0 the Thomas kernel (bit-identical to
-// the sequential restatement): 371 / 382 us.  With FP32 storage the
-// line-major runs shrink to 32 bytes and the staged kernel is faster
-// (290 / 400 us against 305 / 428 us).  Default (-1): 3 for 8-byte values
-// and lines of up to 256 points, 1 otherwise.
+// FP64 y / z solves (CUDA events): 4 the line-major kernel with the warp
+// PCR (trid_lmw_kernel) 147 / 263 us in a stand-alone harness on the ADI
+// driver's layout (258-element rows) where mode 3 took 238 / 382 us, and
+// 173 / 279 us for FP32 storage; 3 the line-major CTA
+// kernel with 8-point chunks and the PCR in shared memory (8 lines x 32
+// chunks per CTA, 64-byte runs, 2 CTAs per SM): 226 / 364 us; 2 the same
+// with 16-point chunks (16 lines, 128-byte runs, 150 registers, 1 CTA per
+// SM): 213 / 438 us; 1 the staged warp-per-line kernel: 300 / 408 us; 0 the
+// Thomas kernel (bit-identical to the sequential restatement): 371 / 382 us.
+// With FP32 storage the line-major runs shrink to 32 bytes and the staged
+// kernel is faster (290 / 400 us against 305 / 428 us).  Default (-1): 4 for
+// lines of up to 256 points, 1 otherwise.
 int strided_mode() {
   static int v = -2;
   if (v == -2) {
@@ -714,15 +1002,30 @@ int strided_mode() {
 }
 bool use_thomas(int unit) { return !unit && strided_mode() == 0; }
 
-// the line-major CTA kernel's chunk length for strided lines, 0: not used
+// the line-major kernel's chunk length for strided lines (-8: the warp-PCR
+// form), 0: not used
 template <typename T>
 int line_major_chunk(const Lines &g) {
   if (g.unit) return 0;
   const int m = strided_mode();
   if (m == 2 && g.n <= 32 * 16) return 16;
   if (m == 3 && g.n <= 32 * 8) return 8;
-  if (m == -1 && sizeof(T) == 8 && g.n <= 32 * 8) return 8;
+  if ((m == 4 || m == -1) && g.n <= 32 * 8) return -8;
   return 0;
+}
+
+// OB2_TRID_UNIT: 1 (default) unit-stride lines of up to 256 points through
+// trid_xw_kernel (vector accesses, 32-bit offsets, three CTAs per SM; the
+// 256^3 x solve in a stand-alone harness: 140 / 161 us FP64 on 16-byte
+// aligned / 258-element rows against 233 / 240 us for trid_warp_kernel,
+// 93 / 142 us FP32 against 166 / 168 us), 0 the kernels below.
+int unit_mode() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("OB2_TRID_UNIT");
+    v = e ? atoi(e) : 1;
+  }
+  return v;
 }
 
 // OB2_TRID_STAGED: 0 never, 1 always, 2 strided lines only (default)
@@ -755,11 +1058,14 @@ int launch(int ndim, int solvedim, const int *dims, const long long *strides, co
   g.unit = g.stride == 1 ? 1 : 0;
   if (g.n <= 0 || g.nlines <= 0) return 0;
   if (use_thomas(g.unit)) return launch_thomas<T>(g, a, b, c, d, u);
+  if (g.unit && g.n <= 32 * 8 && unit_mode() == 1) return launch_xw<T>(g, a, b, c, d, u);
   if (use_pipe<T>(g)) {
     if (g.unit) return launch_pipe<T, false>(g, a, b, c, d, u);
     return launch_pipe<T, true>(g, a, b, c, d, u);
   }
   switch (line_major_chunk<T>(g)) {
+    case -8:
+      return launch_lmw<T>(g, a, b, c, d, u);
     case 8:
       return launch_cta<T, 8, true>(g, a, b, c, d, u);
     case 16:

@@ -29,7 +29,10 @@
 
 namespace {
 
-constexpr int TX = 32;
+constexpr int TX = 32;       // CTA x extent (one warp per row of a tile)
+constexpr int TXC = 2 * TX;  // columns per tile: two adjacent columns per thread
+constexpr int C0 = 2;        // storage column of interior column 0 (even: 2-column
+                             // accesses are 8- or 16-byte aligned)
 constexpr int MAXA = OB2S_MAX_ACTIVE;
 constexpr int ADI_MAX_N = 192;  // x-solve tile: 32 lines x n points in shared memory
 constexpr int ADI_XL = 32;      // lines per x-solve unit
@@ -86,8 +89,13 @@ __device__ __forceinline__ double hash_uniform(int seed, int i, int j, int k) {
 }
 
 // ---------------------------------------------------------------- Poisson
-// CTA 32 x 8 threads; each thread handles RY consecutive rows, so a tile is
-// 32 x (8 RY) points.  Loads of out-of-range rows are clamped to the last
+// Layout of a 2D request's arrays: rows -1 .. n (the zero halo rows) at
+// storage rows 0 .. n+1, row pitch P even and at least n + 3, interior
+// column i at storage column i + C0 (column -1, the left halo, at C0 - 1;
+// column n, the right halo, at n + C0); every unused element is zero.
+// CTA 32 x 8 threads; each thread handles two adjacent columns (one 8- or
+// 16-byte access per array and row) and RY consecutive rows, so a tile is
+// 64 x (8 RY) points.  Loads of out-of-range rows are clamped to the last
 // interior row (always valid memory) and only the stores are guarded, so the
 // loads of all RY rows are issued before any store.
 //
@@ -119,11 +127,29 @@ __device__ __forceinline__ double hash_uniform(int seed, int i, int j, int k) {
 constexpr int CTA_Y = 8;
 constexpr int NPART = 2;  // partial sums per tile: (p', w) and (r, r)
 
-// resident CTAs per SM the Poisson kernels are compiled for (register cap)
+// two adjacent elements of type T
+template <typename T> struct V2;
+template <> struct V2<float> { typedef float2 type; };
+template <> struct V2<double> { typedef double2 type; };
+template <typename T>
+__device__ __forceinline__ typename V2<T>::type ld2(const T *p) {
+  return *(const typename V2<T>::type *)p;
+}
+template <typename T>
+__device__ __forceinline__ void st2(T *p, T a, T b) {
+  typename V2<T>::type v;
+  v.x = a;
+  v.y = b;
+  *(typename V2<T>::type *)p = v;
+}
+
+// resident CTAs per SM the Poisson kernels are compiled for (register cap):
+// 4 for FP32 vectors; 3 for FP64 ones, whose two columns of RY rows need
+// more than 64 registers without spilling
 #ifndef OB2S_MINB
 #define OB2S_MINB 4
 #endif
-#define POIS_BOUNDS __launch_bounds__(256, OB2S_MINB)
+#define POIS_BOUNDS __launch_bounds__(256, sizeof(TI) == 8 ? 3 : OB2S_MINB)
 
 // fixed-order CTA sum of NV values per thread; result in thread 0
 template <int NV>
@@ -159,7 +185,7 @@ __global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
     if (q.done || q.phase != 2) continue;  // uniform over the CTA
     const int t = (int)(un - W->pois_pref[k]);
     const int n = q.n, P = q.pitch;
-    const int i = (t % q.tiles_x) * TX + threadIdx.x;
+    const int i = (t % q.tiles_x) * TXC + 2 * threadIdx.x;  // columns i, i + 1
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
     double v[1] = {0.0};
     if (j0 < n) {  // uniform over the warp (one threadIdx.y per warp)
@@ -168,35 +194,45 @@ __global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
       TI *pout = (TI *)(q.par ? q.p0 : q.p1);
       TI *ww = (TI *)q.w;
       const TI beta = (TI)q.beta;
-      const bool inx = i < n;
-      const int ic = inx ? i : n - 1;  // lanes past the edge load valid memory
+      const bool in0 = i < n, in1 = i + 1 < n;
+      const int ic = in0 ? i : ((n - 1) & ~1);  // lanes past the edge load valid memory
       const int lane = threadIdx.x;
-      // p' = r + beta p on rows j0-1 .. j0+RY of column i (storage rows
+      // p' = r + beta p on rows j0-1 .. j0+RY of columns i, i+1 (storage rows
       // clamped into the array; the halo rows and columns of r and p hold
-      // zeros); a lane past the right edge stands for the zero halo column
-      TI pc[RY + 2];
-      int o[RY + 2];  // (n + 2)^2 < 2^31 for n <= 32768
+      // zeros); a column past the right edge stands for the zero halo
+      TI p0[RY + 2], p1[RY + 2];
+      int o[RY + 2];  // (n + 2) P < 2^31 for n <= 32768
 #pragma unroll
       for (int m = 0; m < RY + 2; m++) {
-        o[m] = (min(j0 + m - 1, n) + 1) * P + (ic + 1);
-        pc[m] = inx ? rr[o[m]] + beta * pin[o[m]] : (TI)0;
+        o[m] = (min(j0 + m - 1, n) + 1) * P + ic + C0;
+        const auto rv = ld2(rr + o[m]);
+        const auto pv = ld2(pin + o[m]);
+        p0[m] = in0 ? rv.x + beta * pv.x : (TI)0;
+        p1[m] = in1 ? rv.y + beta * pv.y : (TI)0;
       }
 #pragma unroll
       for (int m = 0; m < RY; m++) {
-        // west / east neighbours from the adjacent lanes; the warp's edge
-        // lanes form theirs from memory (the same arithmetic, same bits)
-        TI pw = __shfl_up_sync(0xffffffffu, pc[m + 1], 1);
-        TI pe = __shfl_down_sync(0xffffffffu, pc[m + 1], 1);
+        // column i - 1 is the left lane's second column, column i + 2 the
+        // right lane's first; the warp's edge lanes form theirs from memory
+        // (the same arithmetic, same bits)
+        TI pw = __shfl_up_sync(0xffffffffu, p1[m + 1], 1);
+        TI pe = __shfl_down_sync(0xffffffffu, p0[m + 1], 1);
         if (lane == 0) pw = rr[o[m + 1] - 1] + beta * pin[o[m + 1] - 1];
-        if (lane == TX - 1 && inx) pe = rr[o[m + 1] + 1] + beta * pin[o[m + 1] + 1];
-        if (!inx || j0 + m >= n) continue;
-        const TI c = pc[m + 1];
-        const TI a = q.kind == OB2S_HEAT2D
-                         ? (TI)q.diag * c - (TI)q.off * (pw + pe + pc[m] + pc[m + 2])
-                         : (TI)4 * c - pw - pe - pc[m] - pc[m + 2];
-        pout[o[m + 1]] = c;
-        ww[o[m + 1]] = a;
-        v[0] += (double)c * (double)a;
+        if (lane == TX - 1 && in1) pe = rr[o[m + 1] + 2] + beta * pin[o[m + 1] + 2];
+        if (!in0 || j0 + m >= n) continue;
+        const TI c0 = p0[m + 1], c1 = p1[m + 1];
+        TI a0, a1;
+        if (q.kind == OB2S_HEAT2D) {
+          a0 = (TI)q.diag * c0 - (TI)q.off * (pw + c1 + p0[m] + p0[m + 2]);
+          a1 = in1 ? (TI)q.diag * c1 - (TI)q.off * (c0 + pe + p1[m] + p1[m + 2]) : (TI)0;
+        } else {
+          a0 = (TI)4 * c0 - pw - c1 - p0[m] - p0[m + 2];
+          a1 = in1 ? (TI)4 * c1 - c0 - pe - p1[m] - p1[m + 2] : (TI)0;
+        }
+        // column n (the right halo) gets zeros when i + 1 == n
+        st2(pout + o[m + 1], c0, c1);
+        st2(ww + o[m + 1], a0, a1);
+        v[0] += (double)c0 * (double)a0 + (double)c1 * (double)a1;
       }
     }
     block_sum<1>(v, sh);
@@ -205,7 +241,8 @@ __global__ void POIS_BOUNDS pois_pw(const Work *__restrict__ W, Req *R) {
 }
 
 // phase 2: x += alpha p' (FP64), r -= alpha w, (r, r); phases 0, 3:
-// r = b - A x in FP64 and its (r, r)
+// r = b - A x in FP64 and its (r, r).  Column n (the right halo) is written
+// only with zeros: there p', w and r are zero, so x keeps its zero.
 template <typename TI, int RY>
 __global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
   __shared__ double sh[2][32];
@@ -217,13 +254,14 @@ __global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
     const int ph = q.phase;
     const int t = (int)(un - W->pois_pref[k]);
     const int n = q.n, P = q.pitch;
-    const int i = (t % q.tiles_x) * TX + threadIdx.x;
+    const int i = (t % q.tiles_x) * TXC + 2 * threadIdx.x;  // columns i, i + 1
     const int j0 = (t / q.tiles_x) * (CTA_Y * RY) + threadIdx.y * RY;
     double v[2] = {0.0, 0.0};
     if (i < n && j0 < n) {
-      int o[RY];  // (n + 2)^2 < 2^31 for n <= 32768
+      const bool in1 = i + 1 < n;
+      int o[RY];  // (n + 2) P < 2^31 for n <= 32768
 #pragma unroll
-      for (int m = 0; m < RY; m++) o[m] = (min(j0 + m, n - 1) + 1) * P + (i + 1);
+      for (int m = 0; m < RY; m++) o[m] = (min(j0 + m, n - 1) + 1) * P + i + C0;
       TI *rr = (TI *)q.r;
       double *x = q.x;
       if (ph == 2) {
@@ -231,47 +269,55 @@ __global__ void POIS_BOUNDS pois_xr(const Work *__restrict__ W, Req *R) {
         const TI *ww = (const TI *)q.w;
         const double alpha64 = q.alpha;
         const TI alpha = (TI)q.alpha;
-        double xv[RY];
-        TI rv[RY];
+        double x0[RY], x1[RY];
+        TI r0[RY], r1[RY];
 #pragma unroll
         for (int m = 0; m < RY; m++) {
-          const TI pv = pn[o[m]];
-          xv[m] = x[o[m]] + alpha64 * (double)pv;
-          rv[m] = rr[o[m]] - alpha * ww[o[m]];
+          const auto pv = ld2(pn + o[m]);
+          const auto wv = ld2(ww + o[m]);
+          const auto rv = ld2(rr + o[m]);
+          const double2 xv = ld2(x + o[m]);
+          x0[m] = xv.x + alpha64 * (double)pv.x;
+          x1[m] = xv.y + alpha64 * (double)pv.y;
+          r0[m] = rv.x - alpha * wv.x;
+          r1[m] = rv.y - alpha * wv.y;
         }
 #pragma unroll
         for (int m = 0; m < RY; m++) {
           if (j0 + m >= n) continue;
-          x[o[m]] = xv[m];
-          rr[o[m]] = rv[m];
-          v[0] += (double)rv[m] * (double)rv[m];
+          st2(x + o[m], x0[m], x1[m]);
+          st2(rr + o[m], r0[m], r1[m]);
+          v[0] += (double)r0[m] * (double)r0[m] + (double)r1[m] * (double)r1[m];
         }
       } else {
         double *b = q.b;
-        double res[RY];
+        double s0[RY], s1[RY];
 #pragma unroll
         for (int m = 0; m < RY; m++) {
           const int e = o[m];
+          const double2 c = ld2(x + e), up = ld2(x + e - P), dn = ld2(x + e + P);
+          const double xw = x[e - 1], xe = x[e + 2];
+          double2 bv = ld2(b + e);
           if (q.kind == OB2S_HEAT2D) {
-            const double c = x[e];
-            double bv = b[e];
             if (q.newstep) {  // a new time step: its right-hand side is the last solution
               bv = c;
               if (j0 + m < n) {
-                b[e] = bv;
-                v[1] += bv * bv;  // ||b||^2: the step's residuals are relative to it
+                st2(b + e, bv.x, bv.y);
+                v[1] += bv.x * bv.x + bv.y * bv.y;  // ||b||^2: the step's residuals are relative to it
               }
             }
-            res[m] = bv - (q.diag * c - q.off * (x[e - 1] + x[e + 1] + x[e - P] + x[e + P]));
+            s0[m] = bv.x - (q.diag * c.x - q.off * (xw + c.y + up.x + dn.x));
+            s1[m] = in1 ? bv.y - (q.diag * c.y - q.off * (c.x + xe + up.y + dn.y)) : 0.0;
           } else {
-            res[m] = b[e] - (4.0 * x[e] - x[e - 1] - x[e + 1] - x[e - P] - x[e + P]);
+            s0[m] = bv.x - (4.0 * c.x - xw - c.y - up.x - dn.x);
+            s1[m] = in1 ? bv.y - (4.0 * c.y - c.x - xe - up.y - dn.y) : 0.0;
           }
         }
 #pragma unroll
         for (int m = 0; m < RY; m++) {
           if (j0 + m >= n) continue;
-          rr[o[m]] = (TI)res[m];
-          v[0] += res[m] * res[m];
+          st2(rr + o[m], (TI)s0[m], (TI)s1[m]);
+          v[0] += s0[m] * s0[m] + s1[m] * s1[m];
         }
       }
     }
@@ -490,7 +536,7 @@ __global__ void pois_init(double *b, int n, int pitch, int seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= n) return;
   const double h = 1.0 / (n + 1);
-  b[(long long)(j + 1) * pitch + i + 1] = h * h * (2.0 * hash_uniform(seed, i, j, 0) - 1.0);
+  b[(long long)(j + 1) * pitch + i + C0] = h * h * (2.0 * hash_uniform(seed, i, j, 0) - 1.0);
 }
 
 // heat request: u0 ~ U(-1,1) into b and x
@@ -498,8 +544,8 @@ __global__ void heat_init(double *b, double *x, int n, int pitch, int seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= n) return;
   const double v = 2.0 * hash_uniform(seed, i, j, 3) - 1.0;
-  b[(long long)(j + 1) * pitch + i + 1] = v;
-  x[(long long)(j + 1) * pitch + i + 1] = v;
+  b[(long long)(j + 1) * pitch + i + C0] = v;
+  x[(long long)(j + 1) * pitch + i + C0] = v;
 }
 
 __global__ void adi_init(double *u, int n, int seed) {
@@ -508,10 +554,12 @@ __global__ void adi_init(double *u, int n, int seed) {
   u[((long long)z * n + j) * n + i] = 2.0 * hash_uniform(seed, i, j, z + 1) - 1.0;
 }
 
-__global__ void interior_copy(const double *src, double *dst, int n, int pitch, int off) {
+// rows [roff, roff + n) x columns [coff, coff + n) of src into dst (n x n)
+__global__ void interior_copy(const double *src, double *dst, int n, int pitch, int roff,
+                              int coff) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= n) return;
-  dst[(long long)j * n + i] = src[(long long)(j + off) * pitch + i + off];
+  dst[(long long)j * n + i] = src[(long long)(j + roff) * pitch + i + coff];
 }
 
 }  // namespace
@@ -548,8 +596,8 @@ static size_t elem_inner(int mode) { return mode == OB2S_MIXED ? 4 : 8; }
 
 OB2_API size_t ob2s_request_bytes(int mode, int kind, int n) {
   if (kind == OB2S_POISSON2D || kind == OB2S_HEAT2D) {
-    const size_t p = (size_t)(n + 2) * (n + 2);
-    const size_t tiles = (size_t)((n + 31) / 32) * (size_t)((n + 7) / 8);  // at the smallest tile
+    const size_t p = (size_t)((n + 4) & ~1) * (n + 2);  // pitch x rows
+    const size_t tiles = (size_t)((n + TXC - 1) / TXC) * (size_t)((n + 7) / 8);  // smallest tile
     return p * (16 + 4 * elem_inner(mode)) + 8 * NPART * tiles + 4096;
   }
   return (size_t)n * n * n * 16 + (size_t)n * 16 + 4096;
@@ -716,10 +764,10 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
     return (void *)p;
   };
   if (grid2d) {
-    q.pitch = n + 2;
-    q.tiles_x = (n + TX - 1) / TX;
+    q.pitch = (n + 4) & ~1;  // even, >= n + 3: columns 0 .. n + C0
+    q.tiles_x = (n + TXC - 1) / TXC;
     q.tiles = q.tiles_x * ((n + e->tile_y - 1) / e->tile_y);
-    const size_t p = (size_t)q.pitch * q.pitch;
+    const size_t p = (size_t)q.pitch * (n + 2);
     const size_t ei = elem_inner(e->mode);
     // the layout ob2s_request_bytes counts (seven arrays, each rounded up to
     // 256 bytes: within its 4 KB slack)
@@ -877,7 +925,7 @@ OB2_API int ob2s_fetch(ob2s_engine *e, int id, double *host, size_t count) {
     double *tmp = nullptr;
     cudaError_t ce = cudaMallocAsync(&tmp, (size_t)n * n * 8, e->st);
     if (ce != cudaSuccess) return rc(ce);
-    interior_copy<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.x, tmp, n, q.pitch, 1);
+    interior_copy<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.x, tmp, n, q.pitch, 1, C0);
     ce = cudaMemcpyAsync(host, tmp, (size_t)n * n * 8, cudaMemcpyDeviceToHost, e->st);
     cudaFreeAsync(tmp, e->st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);

@@ -184,12 +184,13 @@ def test_trid_thomas_strided_bit_exact(typ, solvedim, inc):
     assert r.returncode == 0, r.stderr[-2000:]
 
 
-@pytest.mark.parametrize("mode", ["1", "2", "3"])
+@pytest.mark.parametrize("mode", ["1", "2", "3", "4"])
 @pytest.mark.parametrize("typ", ["double", "float"])
 def test_trid_strided_kernels(mode, typ):
     """Every kernel for strided lines -- OB2_TRID_STRIDED=1 the staged
     warp-per-line kernel, 2 and 3 the line-major CTA kernel with 16- and
-    8-point chunks -- against the numpy Thomas model: y and z lines, with and
+    8-point chunks, 4 the line-major kernel with the warp PCR -- against the
+    numpy Thomas model: y and z lines, with and
     without _Inc, line counts that do not fill the last CTA, line lengths
     from 5 to 200 (a child process per mode: the choice is read once)."""
     import subprocess
@@ -250,3 +251,25 @@ def test_device_memspace_slab_set_and_fetch():
     assert np.array_equal(slab_out, want[10:12, 10:12].ravel())
     for p in (d_in, d_all, d_slab):
         L.ob2_dev_free(p)
+
+
+@pytest.mark.parametrize("mode", ["0", "1"])
+@pytest.mark.parametrize("typ", ["double", "float"])
+def test_trid_unit_stride_kernels(mode, typ):
+    """Unit-stride (x) lines: OB2_TRID_UNIT=1 the vectorised warp-per-line
+    kernel (16-, 8- or 4-byte accesses as each line's alignment allows, the
+    partial last chunk element by element), 0 the scalar one, against the
+    numpy Thomas model: line lengths 2 to 256 (odd lengths, the halo making
+    every line start off 16-byte alignment), with and without _Inc, line
+    counts that do not fill the last CTA (a child process per mode)."""
+    import subprocess
+    import sys
+    calls = "; ".join("t.test_trid_batch(%r, 0, %r, %r)" % (typ, inc, shape)
+                      for inc in (False, True)
+                      for shape in ((256, 3, 5), (255, 4, 3), (64, 9, 2), (2, 5, 7), (131, 2, 2),
+                                   (300, 2, 2)))
+    code = ("import sys; sys.path.insert(0, %r); import tests.test_gpu_cabi as t; %s" %
+            (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), calls))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       env=dict(os.environ, OB2_TRID_UNIT=mode), timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
