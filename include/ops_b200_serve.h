@@ -79,6 +79,10 @@ typedef struct ob2s_result {
 OB2_API int ob2s_create(ob2s_engine **e, int mode, double tol, double inner_tol, int max_inner,
                         int tile_y);
 OB2_API void ob2s_destroy(ob2s_engine *e);
+/* grows the engine's memory pool to `bytes` once (a server's start-up: the
+ * requests admitted later are carved from memory already mapped instead of
+ * mapping their own); the pool keeps freed memory for the engine's life */
+OB2_API int ob2s_reserve(ob2s_engine *e, size_t bytes);
 /* device bytes a request holds while admitted */
 OB2_API size_t ob2s_request_bytes(int mode, int kind, int n);
 /* Allocates and initialises a request (stream-ordered); it joins the active

@@ -562,6 +562,30 @@ __global__ void interior_copy(const double *src, double *dst, int n, int pitch, 
   dst[(long long)j * n + i] = src[(long long)(j + roff) * pitch + i + coff];
 }
 
+// checksum of a request's solution in a fixed order: CTA c of kSumCtas sums
+// rows [c R / G, (c + 1) R / G) of the R rows of ncols elements (element
+// (i, r) at off + r pitch + i), thread-strided, then block_sum; one CTA sums
+// the partials in order
+constexpr int kSumCtas = 256;
+__global__ void __launch_bounds__(256) sum_rows(const double *src, long long nrows, int ncols,
+                                                long long pitch, long long off, double *part) {
+  __shared__ double sh[1][32];
+  const long long G = gridDim.x, c = blockIdx.x;
+  const long long r0 = nrows * c / G, r1 = nrows * (c + 1) / G;
+  double v[1] = {0.0};
+  for (long long r = r0; r < r1; r++)
+    for (int i = threadIdx.x; i < ncols; i += blockDim.x) v[0] += src[off + r * pitch + i];
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) part[c] = v[0];
+}
+__global__ void __launch_bounds__(256) sum_parts(const double *part, int np, double *out) {
+  __shared__ double sh[1][32];
+  double v[1] = {0.0};
+  for (int k = threadIdx.x; k < np; k += blockDim.x) v[0] += part[k];
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) *out = v[0];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host side
@@ -588,6 +612,11 @@ struct ob2s_engine {
   };
   std::vector<Graph> graphs;
   long long launches;
+  // the requests' memory: a pool of the engine's own that keeps freed
+  // memory mapped (a request admitted after another retired reuses its
+  // pages instead of mapping new ones)
+  cudaMemPool_t pool;
+  double *sum_d;  // checksum scratch: kSumCtas partials and the result
 };
 
 static int rc(cudaError_t e) { return (int)e; }
@@ -689,6 +718,30 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
     }
     e->pois_ctas_per_sm = std::max(1, std::min(nb, nb2));
   }
+  {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    unsigned long long keep = ~0ULL;  // never return freed memory to the device
+    if ((err = cudaMemPoolCreate(&e->pool, &props)) != cudaSuccess) {
+      cudaStreamDestroy(e->st);
+      cudaFree(e->R_d);
+      cudaFree(e->W_d);
+      delete e;
+      return rc(err);
+    }
+    cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if ((err = cudaMalloc(&e->sum_d, sizeof(double) * (kSumCtas + 1))) != cudaSuccess) {
+      cudaMemPoolDestroy(e->pool);
+      cudaStreamDestroy(e->st);
+      cudaFree(e->R_d);
+      cudaFree(e->W_d);
+      delete e;
+      return rc(err);
+    }
+  }
   e->R.assign(MAXA, Req());
   memset(e->R.data(), 0, sizeof(Req) * MAXA);
   e->used.assign(MAXA, 0);
@@ -702,6 +755,20 @@ OB2_API int ob2s_create(ob2s_engine **out, int mode, double tol, double inner_to
   return 0;
 }
 
+OB2_API int ob2s_reserve(ob2s_engine *e, size_t bytes) {
+  if (!e) return OB2S_ERR_BADARG;
+  if (bytes == 0) return 0;
+  void *m = nullptr;
+  cudaError_t err = cudaMallocFromPoolAsync(&m, bytes, e->pool, e->st);
+  if (err != cudaSuccess) {
+    cudaGetLastError();  // too large for the device: not sticky, leave no trace
+    return rc(err);
+  }
+  err = cudaFreeAsync(m, e->st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->st);
+  return rc(err);
+}
+
 OB2_API void ob2s_destroy(ob2s_engine *e) {
   if (!e) return;
   cudaStreamSynchronize(e->st);
@@ -711,6 +778,8 @@ OB2_API void ob2s_destroy(ob2s_engine *e) {
   cudaStreamSynchronize(e->st);
   cudaFree(e->R_d);
   cudaFree(e->W_d);
+  cudaFree(e->sum_d);
+  cudaMemPoolDestroy(e->pool);
   cudaStreamDestroy(e->st);
   delete e;
 }
@@ -747,7 +816,7 @@ OB2_API int ob2s_submit(ob2s_engine *e, int kind, int n, int seed, int steps, in
   if (slot < 0) return OB2S_ERR_FULL;
   const size_t nb = ob2s_request_bytes(e->mode, kind, n);
   void *m = nullptr;
-  cudaError_t err = cudaMallocAsync(&m, nb, e->st);
+  cudaError_t err = cudaMallocFromPoolAsync(&m, nb, e->pool, e->st);
   if (err != cudaSuccess) return rc(err);
   if ((err = cudaMemsetAsync(m, 0, nb, e->st)) != cudaSuccess) {
     cudaFreeAsync(m, e->st);
@@ -923,7 +992,7 @@ OB2_API int ob2s_fetch(ob2s_engine *e, int id, double *host, size_t count) {
   if (q.kind != OB2S_ADI3D) {
     if (count < (size_t)n * n) return OB2S_ERR_BADARG;
     double *tmp = nullptr;
-    cudaError_t ce = cudaMallocAsync(&tmp, (size_t)n * n * 8, e->st);
+    cudaError_t ce = cudaMallocFromPoolAsync(&tmp, (size_t)n * n * 8, e->pool, e->st);
     if (ce != cudaSuccess) return rc(ce);
     interior_copy<<<dim3((n + 127) / 128, n), 128, 0, e->st>>>(q.x, tmp, n, q.pitch, 1, C0);
     ce = cudaMemcpyAsync(host, tmp, (size_t)n * n * 8, cudaMemcpyDeviceToHost, e->st);
@@ -949,12 +1018,17 @@ OB2_API int ob2s_result_of(ob2s_engine *e, int id, ob2s_result *res) {
   res->outer = q.outer;
   res->rel_residual = q.rel;
   if (!q.done) return 0;
-  const size_t m = q.kind != OB2S_ADI3D ? (size_t)q.n * q.n : (size_t)q.n * q.n * q.n;
-  std::vector<double> h(m);
-  int err = ob2s_fetch(e, id, h.data(), m);
-  if (err) return err;
+  const int n = q.n;
+  if (q.kind != OB2S_ADI3D)  // interior rows 1 .. n, columns C0 .. C0 + n - 1
+    sum_rows<<<kSumCtas, 256, 0, e->st>>>(q.x, n, n, q.pitch, (long long)q.pitch + C0, e->sum_d);
+  else
+    sum_rows<<<kSumCtas, 256, 0, e->st>>>(q.u, (long long)n * n, n, n, 0, e->sum_d);
+  sum_parts<<<1, 256, 0, e->st>>>(e->sum_d, kSumCtas, e->sum_d + kSumCtas);
   double s = 0.0;
-  for (size_t i = 0; i < m; i++) s += h[i];
+  cudaError_t ce = cudaMemcpyAsync(&s, e->sum_d + kSumCtas, sizeof(double),
+                                   cudaMemcpyDeviceToHost, e->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->st);
+  if (ce != cudaSuccess) return rc(ce);
   res->checksum = s;
   return 0;
 }

@@ -72,6 +72,7 @@ def lib():
         L.ob2s_result_of.argtypes = [vp, i, ctypes.POINTER(Result)]
         L.ob2s_fetch.argtypes = [vp, i, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]
         L.ob2s_release.argtypes = [vp, i]
+        L.ob2s_reserve.argtypes = [vp, ctypes.c_size_t]
         L.ob2s_launches.argtypes = [vp]
         L.ob2s_launches.restype = ctypes.c_longlong
         L.ob2_error_string.argtypes = [i]
@@ -142,6 +143,20 @@ class Engine:
     def launches(self) -> int:
         return int(lib().ob2s_launches(self.h))
 
+    def reserve(self, nbytes: int) -> None:
+        """Maps nbytes of device memory into the engine's pool once (server
+        start-up), so that admitted requests reuse mapped memory."""
+        check(lib().ob2s_reserve(self.h, nbytes), "ob2s_reserve")
+
+    def reserve_up_to(self, nbytes: int) -> int:
+        """reserve() of nbytes, or of the largest half-step below it that the
+        device can hold; returns the bytes reserved."""
+        while nbytes >= (1 << 28):
+            if lib().ob2s_reserve(self.h, nbytes) == 0:
+                return nbytes
+            nbytes //= 2
+        return 0
+
 
 @dataclass
 class Request:
@@ -200,7 +215,11 @@ def request_bytes_moved(r: Request, mode: int) -> float:
 def serve(engine: Engine, stream: List[Request], budget_bytes: int, iters: int = 16,
           max_active: int = MAX_ACTIVE, keep_solutions: bool = False) -> Dict:
     """Runs the stream through the engine in real time (arrival times are
-    offsets from the start); returns the statistics."""
+    offsets from the start); returns the statistics.  Before the clock
+    starts, the engine's memory pool is grown to the HBM budget once (a
+    server's start-up), so that admitted requests do not map memory."""
+    if hasattr(engine, "reserve_up_to"):
+        engine.reserve_up_to(budget_bytes)
     pending = sorted(stream, key=lambda r: r.arrival)
     queue: List[Request] = []
     running: Dict[int, Request] = {}
