@@ -92,6 +92,8 @@ APPS = {
     # (b200 flavour only: the oracle restates the ACC<> API)
     "ref_tealeaf": ("ref", os.path.join(_REF_ROOT, "apps", "c", "TeaLeaf"), TEALEAF_SRCS, None),
     "ref_mgrid": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mgrid"), ["mgrid.cpp"], None),
+    # complexd dats and an OPS_INC reduction of complexd values
+    "ref_complex": ("ref", os.path.join(_REF_ROOT, "apps", "c", "complex"), ["complex.cpp"], None),
     # the reference's C++ object API test (OPS_CPP_API: OPS_instance methods)
     "ref_multidim_cpp": ("ref", os.path.join(_REF_ROOT, "apps", "c", "multiDim"), ["multidim.cpp"],
                          None),

@@ -116,6 +116,8 @@ OB2_API int ob2_box_copy(char *dat, int type_size, int ncomp, int soa, const int
                          const int *start3, const int *count3, char *buf, int dir);
 
 /* ---- fills ---- */
+/* count values of type_size bytes (1-8, or 16 when both 8-byte halves of
+ * the value are equal, as for complex identities) */
 OB2_API int ob2_fill_value(void *p, const void *val, int type_size, size_t count);
 /* smallest key of a NaN element (key = point * ncomp + component; elements
  * are SoA when soa != 0, AoS otherwise) into *first, or -1 when none;

@@ -42,22 +42,54 @@ template <> struct lim<long long> {
   static __device__ __forceinline__ long long hi() { return LLONG_MAX; }
 };
 
-/* identity of each reduction (ops_lib_core.cpp:840-854) */
+/* identity, combination, lane exchange and volatile read of each reduction
+ * (ops_lib_core.cpp:840-965); complex values (ops_lib_core.cpp:935-952)
+ * have their own rules below */
+template <typename T, int OP> struct red {
+  static __device__ __forceinline__ T identity() {
+    if (OP == OPS_MIN) return lim<T>::hi();
+    if (OP == OPS_MAX) return lim<T>::lo();
+    return T(0);
+  }
+  static __device__ __forceinline__ T combine(T a, T b) {
+    if (OP == OPS_MIN) return b < a ? b : a;
+    if (OP == OPS_MAX) return b > a ? b : a;
+    return a + b;
+  }
+  static __device__ __forceinline__ T shfl_xor(T v, int o) {
+    return __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  static __device__ __forceinline__ T load(const T *p) { return *(const volatile T *)p; }
+};
+/* complex: sums (OPS_INC); the reference starts OPS_MIN at (MAX, MAX) and
+ * OPS_MAX at (0, 0) and defines no order, so only sums are combined */
+template <typename R, int OP> struct red<cuda::std::complex<R>, OP> {
+  typedef cuda::std::complex<R> C;
+  static __device__ __forceinline__ C identity() {
+    return OP == OPS_MIN ? C(lim<R>::hi(), lim<R>::hi()) : C(0, 0);
+  }
+  static __device__ __forceinline__ C combine(C a, C b) { return a + b; }
+  static __device__ __forceinline__ C shfl_xor(C v, int o) {
+    return C(__shfl_xor_sync(0xffffffffu, v.real(), o), __shfl_xor_sync(0xffffffffu, v.imag(), o));
+  }
+  static __device__ __forceinline__ C load(const C *p) {
+    const volatile R *q = (const volatile R *)p;
+    const R re = q[0], im = q[1];
+    return C(re, im);
+  }
+};
+
 template <typename T, int OP> __device__ __forceinline__ T identity() {
-  if (OP == OPS_MIN) return lim<T>::hi();
-  if (OP == OPS_MAX) return lim<T>::lo();
-  return T(0);
+  return red<T, OP>::identity();
 }
 
 template <typename T, int OP> __device__ __forceinline__ T combine(T a, T b) {
-  if (OP == OPS_MIN) return b < a ? b : a;
-  if (OP == OPS_MAX) return b > a ? b : a;
-  return a + b;
+  return red<T, OP>::combine(a, b);
 }
 
 template <typename T, int OP> __device__ __forceinline__ T warp_reduce(T v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = combine<T, OP>(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = combine<T, OP>(v, red<T, OP>::shfl_xor(v, o));
   return v;
 }
 
@@ -114,7 +146,7 @@ __device__ __forceinline__ void final_combine(int dim, const T *part, T *acc, in
   for (int d = 0; d < dim; d++) {
     T v = identity<T, OP>();
     for (int i = t; i < nb; i += nt)
-      v = combine<T, OP>(v, ((const volatile T *)part)[(size_t)i * dim + d]);
+      v = combine<T, OP>(v, red<T, OP>::load(part + (size_t)i * dim + d));
     v = block_reduce<T, OP>(v, sh);
     if (t == 0) acc[d] = first ? v : combine<T, OP>(acc[d], v);
   }

@@ -69,6 +69,25 @@ typedef _Float16 half;
 typedef uint16_t half;
 #endif
 
+/* Complex element types (ops_lib_core.h:95-96 of the reference): std::complex
+ * in host code, libcu++'s cuda::std::complex in code nvcc compiles (the
+ * generated kernels), both two consecutive values, real then imaginary. */
+#ifdef __cplusplus
+#if defined(__CUDACC__)
+#include <cuda/std/complex>
+typedef cuda::std::complex<double> complexd;
+typedef cuda::std::complex<float> complexf;
+#else
+#include <complex>
+typedef std::complex<double> complexd;
+typedef std::complex<float> complexf;
+#endif
+#define ZERO_complexd complexd(0, 0)
+#define INFINITY_complexd complexd(DBL_MAX, DBL_MAX)
+#define ZERO_complexf complexf(0, 0)
+#define INFINITY_complexf complexf(FLT_MAX, FLT_MAX)
+#endif
+
 #ifdef __cplusplus
 #define OPS_EXTERN_C extern "C"
 #else
@@ -462,6 +481,8 @@ inline int type_error(const ull *, const char *t) {
 }
 inline int type_error(const bool *, const char *t) { return strcmp(t, "bool"); }
 inline int type_error(const half *, const char *t) { return strcmp(t, "half"); }
+inline int type_error(const complexd *, const char *t) { return strcmp(t, "complexd"); }
+inline int type_error(const complexf *, const char *t) { return strcmp(t, "complexf"); }
 
 /* ops_lib_core.h:648-694 */
 template <class T>

@@ -366,6 +366,12 @@ OB2_API int ob2_nan_find(const void *p, int ts, int ncomp, int soa, size_t count
 
 OB2_API int ob2_fill_value(void *p, const void *val, int ts, size_t count) {
   if (count == 0) return 0;
+  if (ts == 16) {  // a complex value whose two halves are equal: 2 count 8-byte values
+    if (memcmp(val, (const char *)val + 8, 8) != 0) return (int)cudaErrorInvalidValue;
+    ts = 8;
+    count *= 2;
+  }
+  if (ts > 8 || ts < 1) return (int)cudaErrorInvalidValue;
   unsigned long long v = 0;
   memcpy(&v, val, ts <= 8 ? ts : 8);
   size_t blocks = (count + 255) / 256;

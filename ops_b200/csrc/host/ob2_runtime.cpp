@@ -449,7 +449,20 @@ int type_code(const char *t) {
   if (!strcmp(t, "char")) return 6;
   if (!strcmp(t, "short")) return 7;
   if (!strcmp(t, "long")) return 8;
+  if (!strcmp(t, "complexd")) return 9;
+  if (!strcmp(t, "complexf")) return 10;
   return 0;
+}
+
+/* bytes of one value of type code tc */
+int type_bytes(int tc) {
+  switch (tc) {
+    case 1: case 4: case 8: case 10: return 8;
+    case 6: return 1;
+    case 7: return 2;
+    case 9: return 16;
+    default: return 4;
+  }
 }
 
 /* identity of a reduction / low-dim accumulation (ops_lib_core.cpp:840-965) */
@@ -494,6 +507,18 @@ void identity_bytes(int tc, int acc, void *out, bool lowdim) {
     case 8: {
       long v = acc == OPS_MIN ? LONG_MAX : (acc == OPS_MAX ? LONG_MIN : 0);
       memcpy(out, &v, 8);
+      break;
+    }
+    case 9: {  // complexd: (MAX, MAX) for OPS_MIN, zero otherwise (ops_lib_core.cpp:944-952)
+      double v[2] = {0.0, 0.0};
+      if (acc == OPS_MIN) v[0] = v[1] = DBL_MAX;
+      memcpy(out, v, 16);
+      break;
+    }
+    case 10: {  // complexf (ops_lib_core.cpp:935-943)
+      float v[2] = {0.0f, 0.0f};
+      if (acc == OPS_MIN) v[0] = v[1] = FLT_MAX;
+      memcpy(out, v, 8);
       break;
     }
     default:
@@ -1734,7 +1759,7 @@ OPS_API ops_arg ops_arg_reduce(ops_reduction h, int dim, const char *type, ops_a
     h->initialized = 1;
     h->acc = acc;
     int tc = type_code(type);
-    int ts = tc == 1 || tc == 4 || tc == 8 ? 8 : (tc == 6 ? 1 : (tc == 7 ? 2 : 4));
+    int ts = type_bytes(tc);
     for (int off = 0; off + ts <= h->size; off += ts) identity_bytes(tc, acc, h->data + off, false);
     rt().redx[h->index].pending_first = 1;
   } else if (h->acc != acc) {
@@ -1774,7 +1799,7 @@ OPS_API void ops_reduction_result_char(ops_reduction h, int, char *ptr) {
   } else if (r.dist && h->initialized) {
     // no point of this rank's rows fed the handle: its part is the identity
     const int tc = type_code(h->type);
-    const int ts = tc == 1 || tc == 4 || tc == 8 ? 8 : 4;
+    const int ts = type_bytes(tc);
     for (int k = 0; k + ts <= h->size; k += ts) identity_bytes(tc, h->acc, h->data + k, false);
   }
   if (r.dist) {  // combined over the ranks (the reference's MPI_Allreduce)
@@ -2210,7 +2235,7 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
           dx.edat_prev_acc != a.acc) {
         dx.edat_prev_acc = a.acc;
         ob2_flush();
-        unsigned char idv[8];
+        unsigned char idv[16];
         int tc = type_code(d->type);
         identity_bytes(tc, a.acc, idv, true);
         check(ob2_fill_value(d->data_d, idv, d->type_size, d->mem / d->type_size),
@@ -2584,6 +2609,10 @@ OPS_API void ops_print_dat_to_txtfile(ops_dat d, const char *file) {
       fprintf(f, " %3.10f", ((float *)d->data)[i]);
     else if (!strcmp(d->type, "int"))
       fprintf(f, " %d", ((int *)d->data)[i]);
+    else if (!strcmp(d->type, "complexd"))  // ops_lib_core.cpp:1422-1429
+      fprintf(f, " %3.10lf+%3.10lfi", ((double *)d->data)[2 * i], ((double *)d->data)[2 * i + 1]);
+    else if (!strcmp(d->type, "complexf"))
+      fprintf(f, " %e+%ei", ((float *)d->data)[2 * i], ((float *)d->data)[2 * i + 1]);
     if ((i + 1) % (size_t)(d->size[0] * d->dim) == 0) fprintf(f, "\n");
   }
   fclose(f);

@@ -714,7 +714,7 @@ class Translator:
     ELEM_BYTES = {"double": 8, "long long": 8, "int64_t": 8, "unsigned long long": 8,
                   "float": 4, "int": 4, "unsigned int": 4, "unsigned": 4, "int32_t": 4,
                   "short": 2, "half": 2, "__half": 2, "char": 1, "unsigned char": 1,
-                  "bool": 1}
+                  "bool": 1, "complexd": 16, "complexf": 8}
 
     def light_y_stencil(self, kd) -> bool:
         """True for a short kernel body (OPS_B200_LIGHT statements at most,

@@ -344,7 +344,19 @@ OPS_API ops_arg ops_arg_reduce(ops_reduction h, int dim, const char *type, ops_a
       red_init<int>(h, acc, true);
     else if (!strcmp(type, "long long") || !strcmp(type, "ll"))
       red_init<long long>(h, acc, true);
-    else
+    else if (!strcmp(type, "complexd") || !strcmp(type, "complexf")) {
+      // ops_lib_core.cpp:935-952: OPS_MIN starts at (MAX, MAX), others at 0
+      const bool dbl = type[7] == 'd';
+      const int ts = dbl ? 16 : 8;
+      memset(h->data, 0, h->size);
+      if (acc == OPS_MIN)
+        for (int off = 0; off + ts <= h->size; off += ts) {
+          if (dbl)
+            *(complexd *)(h->data + off) = INFINITY_complexd;
+          else
+            *(complexf *)(h->data + off) = INFINITY_complexf;
+        }
+    } else
       throw OPSException(OPS_NOT_IMPLEMENTED, "Error, reduction type not recognised");
   } else if (h->acc != acc) {
     OPSException ex(OPS_INVALID_ARGUMENT);
@@ -755,6 +767,10 @@ OPS_API void ops_print_dat_to_txtfile(ops_dat d, const char *file) {
       fprintf(f, " %3.10f", ((float *)d->data)[i]);
     else if (!strcmp(d->type, "int"))
       fprintf(f, " %d", ((int *)d->data)[i]);
+    else if (!strcmp(d->type, "complexd"))  // ops_lib_core.cpp:1422-1429
+      fprintf(f, " %3.10lf+%3.10lfi", ((double *)d->data)[2 * i], ((double *)d->data)[2 * i + 1]);
+    else if (!strcmp(d->type, "complexf"))
+      fprintf(f, " %e+%ei", ((float *)d->data)[2 * i], ((float *)d->data)[2 * i + 1]);
     if ((i + 1) % (size_t)(d->size[0] * d->dim) == 0) fprintf(f, "\n");
   }
   fclose(f);

@@ -266,6 +266,23 @@ def test_reference_mgrid_known_answer_on_b200():
     assert "PASSED" in out and "FAILED" not in out, out[-1500:]
 
 
+def test_reference_complex_on_b200():
+    """The reference's complex test (apps/c/complex, OPS_ACCn kernels)
+    built unchanged: a complexd dat filled with (x, y) from ops_arg_idx and
+    an OPS_INC reduction of complexd values; its own check is the exact sum
+    90 + 90i, and the dat written by ops_print_dat_to_txtfile holds the same
+    values (the interior 6 x 6 points, in the reference's complex format)."""
+    d = tempfile.mkdtemp(prefix="complex_")
+    out = run_exe("ref_complex", "b200", cwd=d)
+    assert "reduction result: 90+90i" in out and "PASSED" in out, out[-1500:]
+    txt = open(os.path.join(d, "data.txt")).read().split("\n")
+    rows = [l.split() for l in txt[1:] if l.strip()]
+    # storage rows -2 .. 7 (halo depth 2); interior point (x, y) = x + y i
+    for y in range(6):
+        for x in range(6):
+            assert rows[y + 2][x + 2] == "%.10f+%.10fi" % (x, y), (x, y, rows[y + 2][x + 2])
+
+
 def test_reference_cpp_object_api_multidim_on_b200():
     """The reference's C++ object API test (apps/c/multiDim: OPS_instance
     created by the application with its own output stream, SoA storage set on

@@ -57,6 +57,7 @@ def test_cloverleaf_3840_matches_reference_openmp(tmp_path):
         res[fl] = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
     try:
         diffs = check(dumps["b200"], dumps["ref_omp"])
+        print("PARITY cloverleaf_3840 per element", json.dumps(diffs, sort_keys=True))
         assert len(diffs) == 35
     finally:
         for p in dumps.values():
@@ -85,6 +86,8 @@ def test_adi_256_matches_oracle(prec, tmp_path):
         for name, d in diffs.items():
             assert d <= (1e-6 if meta[name][0]["type"] == "float" else 1e-12), (name, d)
         dd = compare(gd, cd, mmap=True, floor_frac=1.0)
+        print("PARITY adi_256 prec %s per element" % prec, json.dumps(diffs, sort_keys=True),
+              "relative to scale", json.dumps(dd, sort_keys=True))
         for name, d in dd.items():
             if name.startswith("du_"):
                 assert d <= (1e-6 if meta[name][0]["type"] == "float" else 1e-12), (name, d)
@@ -125,8 +128,8 @@ def test_heat_cg_4096_matches_reference_seq(prec, tmp_path):
         for p in (gd, cd):
             if os.path.exists(p):
                 os.unlink(p)
-    print("per element", per_elem)
-    print("relative to scale", scale)
+    print("PARITY heat_cg_4096 prec %s per element" % prec, json.dumps(per_elem, sort_keys=True),
+          "relative to scale", json.dumps(scale, sort_keys=True))
     for name in ("density", "u0", "Kx", "Ky", "Kx32", "Ky32"):
         if name in per_elem:
             assert per_elem[name] == 0.0, (name, per_elem[name])
