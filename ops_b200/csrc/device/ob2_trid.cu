@@ -234,6 +234,14 @@ __device__ __forceinline__ void load8(const T *p, double (&v)[8]) {
         const float2 t = ((const float2 *)q)[i];
         v[2 * i] = t.x; v[2 * i + 1] = t.y;
       }
+    } else if ((ad & 7) == 4) {  // one element, three 8-byte pairs, one element
+      v[0] = q[0];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const float2 t = ((const float2 *)(q + 1))[i];
+        v[2 * i + 1] = t.x; v[2 * i + 2] = t.y;
+      }
+      v[7] = q[7];
     } else {
 #pragma unroll
       for (int i = 0; i < 8; i++) v[i] = q[i];
@@ -266,6 +274,12 @@ __device__ __forceinline__ void store8(T *p, const double (&v)[8]) {
     } else if ((ad & 7) == 0) {
 #pragma unroll
       for (int i = 0; i < 4; i++) ((float2 *)q)[i] = make_float2((float)v[2 * i], (float)v[2 * i + 1]);
+    } else if ((ad & 7) == 4) {
+      q[0] = (float)v[0];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        ((float2 *)(q + 1))[i] = make_float2((float)v[2 * i + 1], (float)v[2 * i + 2]);
+      q[7] = (float)v[7];
     } else {
 #pragma unroll
       for (int i = 0; i < 8; i++) q[i] = (float)v[i];
@@ -983,7 +997,9 @@ bool use_pipe(const Lines &g) {
 // FP64 y / z solves (CUDA events): 4 the line-major kernel with the warp
 // PCR (trid_lmw_kernel) 147 / 263 us in a stand-alone harness on the ADI
 // driver's layout (258-element rows) where mode 3 took 238 / 382 us, and
-// 173 / 279 us for FP32 storage; 3 the line-major CTA
+// 173 / 279 us for FP32 storage (16 lines per CTA instead of 8, for
+// 64-byte runs, one CTA per SM: y / z 194 / 309 us FP64, 259 / 375 us FP32
+// in the application, against 150 / 267 and 179 / 286); 3 the line-major CTA
 // kernel with 8-point chunks and the PCR in shared memory (8 lines x 32
 // chunks per CTA, 64-byte runs, 2 CTAs per SM): 226 / 364 us; 2 the same
 // with 16-point chunks (16 lines, 128-byte runs, 150 registers, 1 CTA per
