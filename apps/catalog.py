@@ -59,8 +59,11 @@ APPS = {
     "adi3d": ("own", os.path.join(ROOT, "apps", "adi3d"), ["adi3d.cpp"], None),
     "heat_cg": ("own", os.path.join(ROOT, "apps", "heat_cg"), ["heat_cg.cpp"], None),
     "opsunit": ("own", os.path.join(ROOT, "apps", "opsunit"), ["opsunit.cpp"], None),
+    "hdunit": ("own", os.path.join(ROOT, "apps", "hdunit"), ["hdunit.cpp"], None),
     "ref_poisson": ("ref", os.path.join(_REF_ROOT, "apps", "c", "poisson"), ["poisson.cpp"], None),
     "ref_mblock": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mblock"), ["mblock.cpp"], None),
+    # 4D blocks: two 4^4 blocks filled from ops_arg_idx, joined by a 4D halo
+    "ref_mblock4d": ("ref", os.path.join(_REF_ROOT, "apps", "c", "mblock4D"), ["mblock.cpp"], None),
     "ref_laplace": ("ref", os.path.join(_REF_ROOT, "apps", "c", "laplace2d_tutorial", "step7"),
                     ["laplace2d.cpp"], None),
     # further reference applications, built unchanged (the v2 ACC API)

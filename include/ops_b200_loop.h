@@ -24,6 +24,10 @@ typedef struct ob2_view {
   char *base;
   long long wx, wy, wz;
   int ex, ey, ez, ed;
+  /* 4D / 5D blocks: the walk and the ACC strides along the 4th and 5th axes
+   * (element of point (x,y,z,u,v) = base + x*wx + y*wy + z*wz + u*wu + v*wv) */
+  long long wu, wv;
+  int eu, ev;
 } ob2_view;
 
 /* reduction target of one ops_arg_reduce */
@@ -133,6 +137,10 @@ typedef struct ob2_loop {
                                in the parameter block (tfn != NULL) */
   const int *tb_role;       /* per argument: 1 a read dat the chain may
                                ping-pong, 2 the written dat, 0 other */
+  int lo4[2], hi4[2];       /* 4D / 5D blocks: the range along the 4th and
+                               5th axes (0 / 1 for fewer dimensions); the
+                               suggested grid's z extent covers the product
+                               of the extents along the 3rd to 5th axes */
 } ob2_loop;
 
 /* A generated launcher: launches one kernel variant with the parameter block

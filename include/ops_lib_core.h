@@ -613,10 +613,15 @@ template <typename T> class ACC {
   int sy;    /* elements between neighbouring y points */
   int sz;    /* elements between neighbouring z points */
   int sd;    /* elements between components */
+  int su;    /* elements between neighbouring points along the 4th axis */
+  int sv;    /* elements between neighbouring points along the 5th axis */
 
-  __host__ __device__ __forceinline__ ACC() : p(0), sx(1), sy(0), sz(0), sd(1) {}
+  __host__ __device__ __forceinline__ ACC() : p(0), sx(1), sy(0), sz(0), sd(1), su(0), sv(0) {}
   __host__ __device__ __forceinline__ ACC(T *ptr, int sx_, int sy_, int sz_, int sd_)
-      : p(ptr), sx(sx_), sy(sy_), sz(sz_), sd(sd_) {}
+      : p(ptr), sx(sx_), sy(sy_), sz(sz_), sd(sd_), su(0), sv(0) {}
+  __host__ __device__ __forceinline__ ACC(T *ptr, int sx_, int sy_, int sz_, int su_, int sv_,
+                                          int sd_)
+      : p(ptr), sx(sx_), sy(sy_), sz(sz_), sd(sd_), su(su_), sv(sv_) {}
   __host__ __device__ __forceinline__ void next(long elems) { p += elems; }
 
   /* accumulation into shared points (low-dim dats): atomic on the device */
@@ -642,7 +647,27 @@ template <typename T> class ACC {
 #endif
   }
 
-#if defined(OPS_1D)
+#if defined(OPS_5D)
+  __host__ __device__ __forceinline__ void combine_inc(int x, int y, int z, int u, int w, T v) const {
+    acc_inc(&p[x * sx + y * sy + z * sz + u * su + w * sv], v);
+  }
+  __host__ __device__ __forceinline__ void combine_min(int x, int y, int z, int u, int w, T v) const {
+    acc_min(&p[x * sx + y * sy + z * sz + u * su + w * sv], v);
+  }
+  __host__ __device__ __forceinline__ void combine_max(int x, int y, int z, int u, int w, T v) const {
+    acc_max(&p[x * sx + y * sy + z * sz + u * su + w * sv], v);
+  }
+#elif defined(OPS_4D)
+  __host__ __device__ __forceinline__ void combine_inc(int x, int y, int z, int u, T v) const {
+    acc_inc(&p[x * sx + y * sy + z * sz + u * su], v);
+  }
+  __host__ __device__ __forceinline__ void combine_min(int x, int y, int z, int u, T v) const {
+    acc_min(&p[x * sx + y * sy + z * sz + u * su], v);
+  }
+  __host__ __device__ __forceinline__ void combine_max(int x, int y, int z, int u, T v) const {
+    acc_max(&p[x * sx + y * sy + z * sz + u * su], v);
+  }
+#elif defined(OPS_1D)
   __host__ __device__ __forceinline__ void combine_inc(int x, T v) const { acc_inc(&p[x * sx], v); }
   __host__ __device__ __forceinline__ void combine_min(int x, T v) const { acc_min(&p[x * sx], v); }
   __host__ __device__ __forceinline__ void combine_max(int x, T v) const { acc_max(&p[x * sx], v); }
@@ -668,7 +693,22 @@ template <typename T> class ACC {
   }
 #endif
 
-#if defined(OPS_1D)
+#if defined(OPS_5D)
+  __host__ __device__ __forceinline__ T &operator()(int x, int y, int z, int u, int w) const {
+    return p[x * sx + y * sy + z * sz + u * su + w * sv];
+  }
+  __host__ __device__ __forceinline__ T &operator()(int d, int x, int y, int z, int u,
+                                                    int w) const {
+    return p[d * sd + x * sx + y * sy + z * sz + u * su + w * sv];
+  }
+#elif defined(OPS_4D)
+  __host__ __device__ __forceinline__ T &operator()(int x, int y, int z, int u) const {
+    return p[x * sx + y * sy + z * sz + u * su];
+  }
+  __host__ __device__ __forceinline__ T &operator()(int d, int x, int y, int z, int u) const {
+    return p[d * sd + x * sx + y * sy + z * sz + u * su];
+  }
+#elif defined(OPS_1D)
   __host__ __device__ __forceinline__ T &operator()(int x) const { return p[x * sx]; }
   __host__ __device__ __forceinline__ T &operator()(int d, int x) const {
     return p[d * sd + x * sx];

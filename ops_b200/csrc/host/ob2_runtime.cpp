@@ -690,7 +690,7 @@ void run_tiled(std::vector<Runtime::QItem> &q, size_t b, size_t e) {
 }
 
 bool tileable(const Runtime::QItem &it) {
-  if (it.kind != 0 || it.ndim < 2) return false;
+  if (it.kind != 0 || it.ndim < 2 || it.ndim > 3) return false;  // 4D / 5D: untiled
   for (auto &a : it.acc) {
     if (a.flat && a.acc != OPS_READ) return false;  // shared across tiles
     if (a.mg) return false;  // multigrid: the dat's rows are not the loop's
@@ -1537,9 +1537,9 @@ OPS_API void ops_exit(void) {
 OPS_API void ops_set_soa(const int soa) { I().OPS_soa = soa; }
 
 OPS_API ops_block ops_decl_block(int dims, const char *name) {
-  if (dims < 1 || dims > 3)
+  if (dims < 1 || dims > OPS_MAX_DIM)
     throw OPSException(OPS_INVALID_ARGUMENT,
-                       "Error: ops_decl_block -- this backend supports 1D, 2D and 3D blocks");
+                       "Error: ops_decl_block -- this backend supports 1D to 5D blocks");
   ops_block b = (ops_block)calloc(1, sizeof(ops_block_core));
   b->dims = dims;
   b->name = copy_str(name);
@@ -1918,9 +1918,16 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
   gx.dhi.clear();
   for (int hh = 0; hh < g->nhalos; hh++) {
     ops_halo h = g->halos[hh];
-    for (int i = 3; i < OPS_MAX_DIM; i++)
-      if (h->iter_size[i] != 1)
-        throw OPSException(OPS_NOT_IMPLEMENTED, "Error: halos above 3D are not supported");
+    // 4D / 5D blocks: the box is cut into 3D boxes, one per index along the
+    // 4th and 5th axes, which must map onto themselves (flips allowed)
+    int hi_iter[2] = {1, 1};
+    for (int i = 3; i < OPS_MAX_DIM; i++) {
+      hi_iter[i - 3] = h->iter_size[i];
+      if (h->iter_size[i] != 1 &&
+          (abs(h->from_dir[i]) != i + 1 || abs(h->to_dir[i]) != i + 1))
+        throw OPSException(OPS_NOT_IMPLEMENTED,
+                           "Error: a halo whose 4th or 5th axis maps onto another axis");
+    }
     if (h->from->dim != h->to->dim)
       throw OPSException(OPS_INVALID_ARGUMENT,
                          "Error: ops_halo_transfer between dats of different dim");
@@ -1978,20 +1985,52 @@ static void build_halo_tasks(ops_halo_group g, GroupX &gx) {
       }
     }
     if (t.npts > gx.max_pts) gx.max_pts = t.npts;
-    {
-      std::array<int, 3> og, lo, hi;
-      for (int i = 0; i < 3; i++) {
-        og[i] = h->to->d_m[i] + h->to->base[i];
-        lo[i] = og[i] + t.dst_start[i];
-        hi[i] = lo[i] + t.iter[t.dst_axis[i]];
-      }
-      gx.org.push_back(og);
-      gx.dlo.push_back(lo);
-      gx.dhi.push_back(hi);
-      gx.src_dat.push_back(h->from->index);
-      gx.dst_dat.push_back(h->to->index);
+    // storage index and point offset along the 4th and 5th axes
+    long long hstart[2][2], hcum[2][2];
+    for (int i = 3; i < OPS_MAX_DIM; i++) {
+      hstart[0][i - 3] = h->from_base[i] - h->from->d_m[i] - h->from->base[i];
+      hstart[1][i - 3] = h->to_base[i] - h->to->d_m[i] - h->to->base[i];
+      hcum[0][i - 3] = fc;
+      hcum[1][i - 3] = tc;
+      fc *= h->from->size[i];
+      tc *= h->to->size[i];
+      if (hi_iter[i - 3] != 1 &&
+          (hstart[0][i - 3] < 0 || hstart[0][i - 3] + hi_iter[i - 3] > h->from->size[i] ||
+           hstart[1][i - 3] < 0 || hstart[1][i - 3] + hi_iter[i - 3] > h->to->size[i]))
+        throw OPSException(OPS_INVALID_ARGUMENT, "Error: halo reaches outside its dats");
     }
-    tasks.push_back(t);
+    t.src_npts_total = fc;  // all axes: the component stride of SoA dats
+    t.dst_npts_total = tc;
+    for (int a4 = 0; a4 < hi_iter[1]; a4++)
+      for (int a3 = 0; a3 < hi_iter[0]; a3++) {
+        ob2_halo_task u = t;
+        const int hi_a[2] = {a3, a4};
+        long long soff = 0, doff = 0;
+        for (int k = 0; k < 2; k++) {
+          if (hi_iter[k] == 1 && h->iter_size[3 + k] == 1 &&
+              h->from->block->dims <= 3 + k)
+            continue;
+          const int fi = h->from_dir[3 + k] < 0 ? hi_iter[k] - 1 - hi_a[k] : hi_a[k];
+          const int ti = h->to_dir[3 + k] < 0 ? hi_iter[k] - 1 - hi_a[k] : hi_a[k];
+          soff += (hstart[0][k] + fi) * hcum[0][k];
+          doff += (hstart[1][k] + ti) * hcum[1][k];
+        }
+        // AoS: ncomp values per point; SoA: components npts_total apart
+        u.src += soff * (u.src_soa ? 1 : u.ncomp) * u.src_type;
+        u.dst += doff * (u.dst_soa ? 1 : u.ncomp) * u.dst_type;
+        std::array<int, 3> og, lo, hi;
+        for (int i = 0; i < 3; i++) {
+          og[i] = h->to->d_m[i] + h->to->base[i];
+          lo[i] = og[i] + u.dst_start[i];
+          hi[i] = lo[i] + u.iter[u.dst_axis[i]];
+        }
+        gx.org.push_back(og);
+        gx.dlo.push_back(lo);
+        gx.dhi.push_back(hi);
+        gx.src_dat.push_back(h->from->index);
+        gx.dst_dat.push_back(h->to->index);
+        tasks.push_back(u);
+      }
     gx.key.push_back(h->from->data_d);
     gx.key.push_back(h->to->data_d);
   }
@@ -2012,7 +2051,7 @@ OPS_API void ops_halo_transfer(ops_halo_group g) {
   require_init();
   if (rt().dist) dist_unsupported(nullptr, "ops_halo_transfer between blocks");
   GroupX &gx = rt().groupx[g->index];
-  bool stale = gx.ntasks != g->nhalos || gx.key.size() != (size_t)2 * g->nhalos;
+  bool stale = gx.key.size() != (size_t)2 * g->nhalos;
   for (int hh = 0; !stale && hh < g->nhalos; hh++)
     stale = gx.key[2 * hh] != g->halos[hh]->from->data_d ||
             gx.key[2 * hh + 1] != g->halos[hh]->to->data_d;
@@ -2171,9 +2210,15 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   L->args = args;
   L->stream = ob2_dev_stream();
   L->npoints = 1;
+  if (dim < 1 || dim > OPS_MAX_DIM)
+    throw OPSException(OPS_INVALID_ARGUMENT, "Error: ops_par_loop dimension out of range");
   for (int i = 0; i < 3; i++) {
     L->lo[i] = i < dim ? range[2 * i] : 0;
     L->hi[i] = i < dim ? range[2 * i + 1] : 1;
+  }
+  for (int i = 0; i < 2; i++) {  // the 4th and 5th axes of 4D / 5D blocks
+    L->lo4[i] = 3 + i < dim ? range[2 * (3 + i)] : 0;
+    L->hi4[i] = 3 + i < dim ? range[2 * (3 + i) + 1] : 1;
   }
   if (r.dist) dist_loop(block, dim, L->lo, L->hi, args, nargs, name);
   // a loop launched at once (reductions, autotuning) runs the queue first:
@@ -2190,6 +2235,16 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
     L->n[i] = std::max(0, L->hi[i] - L->lo[i]);
     L->npoints *= L->n[i];
   }
+  // 4D / 5D: the generated kernel walks the 3rd to 5th axes as one folded
+  // index, so the grid's z extent covers their product
+  long long nfold = L->n[2];
+  for (int i = 0; i < 2; i++) {
+    const long long e = std::max(0, L->hi4[i] - L->lo4[i]);
+    L->npoints *= e;
+    nfold *= e;
+  }
+  if (nfold > 0x7fffffffLL)
+    throw OPSException(OPS_NOT_IMPLEMENTED, "Error: ops_par_loop range too large");
   L->kernel_index = kernel_slot(name);
   L->block[0] = r.block_x;
   L->block[1] = dim > 1 ? r.block_y : 1;
@@ -2259,32 +2314,42 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
         throw ex;
       }
       long long cum = 1, off = 0;
-      long long step[3] = {0, 0, 0};
-      for (int k = 0; k < block->dims && k < 3; k++) {
+      long long step[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
+      long long cums[OPS_MAX_DIM + 1] = {1, 1, 1, 1, 1, 1};  // points before axis k
+      for (int k = 0; k < block->dims && k < OPS_MAX_DIM; k++) {
         int sk = st ? st[k] : 1;
         if (stype == 2) sk *= a.stencil->mgrid_stride[k];  // restrict: index * stride
         off += cum * (long long)(-d->base[k] - d->d_m[k]);
         step[k] = cum * sk;
+        cums[k] = cum;
         cum *= d->size[k];
       }
       if (soa) {
         v.ex = 1;
         v.ey = d->size[0];
         v.ez = d->size[0] * d->size[1];
+        v.eu = (int)cums[3];
+        v.ev = (int)cums[4];
         v.ed = (int)cum;
         v.base = d->data_d + off * d->type_size;
         v.wx = step[0];
         v.wy = step[1];
         v.wz = step[2];
+        v.wu = step[3];
+        v.wv = step[4];
       } else {
         v.ex = md;
         v.ey = d->size[0] * md;
         v.ez = d->size[0] * d->size[1] * md;
+        v.eu = (int)(cums[3] * md);
+        v.ev = (int)(cums[4] * md);
         v.ed = 1;
         v.base = d->data_d + off * d->elem_size;
         v.wx = step[0] * md;
         v.wy = step[1] * md;
         v.wz = step[2] * md;
+        v.wu = step[3] * md;
+        v.wv = step[4] * md;
       }
     } else if (a.argtype == OPS_ARG_GBL && a.acc != OPS_READ) {
       ops_reduction h = (ops_reduction)a.data;
@@ -2307,14 +2372,14 @@ OPS_API int ob2_loop_begin(ob2_loop *L, const char *name, ops_block block, int d
   // grid: x covers the range; y and z are capped so that the grid is about
   // one wave of resident CTAs (SMs x CTAs per SM), threads loop over the rest
   L->tune = -1;
-  if (r.autotune && nred == 0 && dim >= 2) tune_pick(L);
+  if (r.autotune && nred == 0 && dim >= 2 && dim <= 3) tune_pick(L);
   {
     long long tpb = (long long)L->block[0] * L->block[1] * L->block[2];
     long long per_sm = std::max(1LL, 2048 / tpb);
     long long target = (long long)r.sms * per_sm * r.red_waves;
     long long gx = (L->n[0] + L->block[0] - 1) / L->block[0];
     long long gy = (L->n[1] + L->block[1] - 1) / L->block[1];
-    long long gz = (L->n[2] + L->block[2] - 1) / L->block[2];
+    long long gz = (nfold + L->block[2] - 1) / L->block[2];
     if (nred > 0) {  // reduction kernels stride over y/z (see the generated kernel)
       long long cy = std::max(1LL, target / std::max(1LL, gx));
       if (gy > cy) gy = cy;
@@ -2729,6 +2794,9 @@ static void stage_reserve(size_t n) {
 /* packed AoS slab <-> dat: dir 0 fetch, 1 set (ops_util.cpp:353-500) */
 static void slab_io(ops_dat d, char *data, const int *range, ops_memspace ms, int dir) {
   require_init();
+  if (d->block->dims > 3)
+    throw OPSException(OPS_NOT_IMPLEMENTED,
+                       "Error: slab fetch / set of a dat of a 4D or 5D block");
   int start[3] = {0, 0, 0}, count[3] = {1, 1, 1}, size3[3] = {1, 1, 1};
   size_t pts = 1;
   for (int i = 0; i < 3; i++) size3[i] = d->size[i];

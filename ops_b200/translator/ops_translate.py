@@ -890,14 +890,21 @@ class Translator:
         nd = loop.ndim
         P = "ob2p_" + loop.stub[len("ops_par_loop_"):]
         K = "ob2k_" + loop.stub[len("ops_par_loop_"):]
+        hd = nd >= 4  # 4D / 5D block: the 4th and 5th axes fold into the grid's z
+        if hd and not all(p.is_acc for a, p in zip(loop.args, kd.params) if a.kind == "dat"):
+            raise SystemExit("%s: %dD loops need ACC<> kernel parameters" % (loop.kernel, nd))
         w("struct %s {" % P)
         w("  int lo0, lo1, lo2, hi0, hi1, hi2;")
         w("  unsigned int *counter;")
+        if hd:
+            w("  int lo3, hi3, lo4, hi4;")
         reds = []
         for i, (a, p) in enumerate(zip(loop.args, kd.params)):
             if a.kind == "dat":
                 w("  %s *b%d; long long wx%d, wy%d, wz%d; int ex%d, ey%d, ez%d, ed%d;" %
                   (p.base_type, i, i, i, i, i, i, i, i))
+                if hd:
+                    w("  long long wu%d, wv%d; int eu%d, ev%d;" % (i, i, i, i))
                 if a.prolong:  # multigrid stride: the loop index is divided by it
                     w("  int mx%d, my%d, mz%d;" % (i, i, i))
                 if self.check:
@@ -920,8 +927,8 @@ class Translator:
             # IDX32: element offsets in 32-bit arithmetic (every dat of the
             # launch has fewer than 2^31 elements; decided by the runtime)
             w("template <bool IDX32>")
-            w("static __device__ __forceinline__ void %s_%s(const %s &p, int x, int y, int z%s) {" %
-              (I, variant, P, prm))
+            w("static __device__ __forceinline__ void %s_%s(const %s &p, int x, int y, int z%s%s) {" %
+              (I, variant, P, ", int u, int v" if hd else "", prm))
             call = []
             for i, (a, p) in enumerate(zip(loop.args, kd.params)):
                 if a.kind == "dat":
@@ -930,13 +937,22 @@ class Translator:
                         cx, cy, cz = ("(x / p.mx%d)" % i, "(y / p.my%d)" % i, "(z / p.mz%d)" % i)
                     else:
                         cx, cy, cz = "x", "y", "z"
-                    off = ("(IDX32 ? (long long)(%s * (int)p.wx%d + %s * (int)p.wy%d + %s * (int)p.wz%d)"
-                           " : %s * p.wx%d + %s * p.wy%d + %s * p.wz%d)" %
-                           (cx, i, cy, i, cz, i, cx, i, cy, i, cz, i))
+                    if hd:
+                        off = ("(IDX32 ? (long long)(x * (int)p.wx%d + y * (int)p.wy%d + z * (int)p.wz%d"
+                               " + u * (int)p.wu%d + v * (int)p.wv%d) : x * p.wx%d + y * p.wy%d"
+                               " + z * p.wz%d + u * p.wu%d + v * p.wv%d)" %
+                               (i, i, i, i, i, i, i, i, i, i))
+                    else:
+                        off = ("(IDX32 ? (long long)(%s * (int)p.wx%d + %s * (int)p.wy%d + %s * (int)p.wz%d)"
+                               " : %s * p.wx%d + %s * p.wy%d + %s * p.wz%d)" %
+                               (cx, i, cy, i, cz, i, cx, i, cy, i, cz, i))
                     # only optional arguments can carry a null dat
                     ptr = ("q%d ? q%d + %s : (%s *)0" % (i, i, off, p.base_type)) if a.opt \
                         else "q%d + %s" % (i, off)
-                    if p.is_acc:
+                    if p.is_acc and hd:
+                        w("  ACC<%s> a%d(%s, %s, p.ey%d, p.ez%d, p.eu%d, p.ev%d, p.ed%d);" %
+                          (p.base_type, i, ptr, ex, i, i, i, i, i))
+                    elif p.is_acc:
                         w("  ACC<%s> a%d(%s, %s, p.ey%d, p.ez%d, p.ed%d);" %
                           (p.base_type, i, ptr, ex, i, i, i))
                     else:  # OPS_ACCn kernel: the point's pointer (strides below)
@@ -951,7 +967,10 @@ class Translator:
                 elif a.kind == "idx":
                     call.append("idx")
             if any(a.kind == "idx" for a in loop.args):
-                w("  int idx[3] = {x, y, z};")
+                if hd:
+                    w("  int idx[%d] = {x, y, z, u%s};" % (nd, ", v" if nd >= 5 else ""))
+                else:
+                    w("  int idx[3] = {x, y, z};")
             for i, (a, p) in enumerate(zip(loop.args, kd.params)):
                 if a.kind == "dat" and not p.is_acc:
                     ex = "1" if a.dim.strip() == "1" else "p.ex%d" % i
@@ -967,7 +986,7 @@ class Translator:
                         call.append("p.clo%d - %s, p.chi%d - %s" % (i, po, i, po))
             w("  %s(%s);" % (loop.kernel, ", ".join(call)))
             w("}")
-        py = self.rows_per_thread(dats, kd)
+        py = 1 if hd else self.rows_per_thread(dats, kd)
         aw = self.align_dat(loop, kd, dats, reds, py)
         if aw is not None:
             w("template <bool RESTRICT, bool IDX32, bool ALIGN = true>")
@@ -1002,33 +1021,56 @@ class Translator:
             # together
             w("  if (x < p.hi0) {")
             w("    const int ys = (int)(gridDim.y * blockDim.y) * %d;" % py)
-            w("    for (int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z); z < p.hi2;"
-              " z += (int)(gridDim.z * blockDim.z))")
+            if hd:  # the 3rd to 5th axes as one folded index
+                w("    const int nz = p.hi2 - p.lo2, nu = p.hi3 - p.lo3, nzu = nz * (p.hi4 - p.lo4) * nu;")
+                w("    for (int zz = (int)(bz * blockDim.z + threadIdx.z); zz < nzu;"
+                  " zz += (int)(gridDim.z * blockDim.z)) {")
+                w("      const int z = p.lo2 + zz % nz, u = p.lo3 + (zz / nz) % nu,"
+                  " v = p.lo4 + zz / (nz * nu);")
+            else:
+                w("    for (int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z); z < p.hi2;"
+                  " z += (int)(gridDim.z * blockDim.z))")
             w("      for (int yb = p.lo1 + (int)(by * blockDim.y + threadIdx.y) * %d;"
               " yb < p.hi1; yb += ys) {" % py)
             # PY consecutive rows per trip; all in range: no branch between
             # the calls, so the loads of every row can be issued before the
             # stores of the first, and rows shared by the stencils are loaded
             # once
+            zc = "z, u, v" if hd else "z"
             w("        if (yb + %d < p.hi1) {" % (py - 1))
             w("#pragma unroll")
             w("          for (int j = 0; j < %d; j++) {" % py)
-            w("            if (RESTRICT) %s_R<IDX32>(p, x, yb + j, z%s);" % (I, args_call))
-            w("            else %s_A<IDX32>(p, x, yb + j, z%s);" % (I, args_call))
+            w("            if (RESTRICT) %s_R<IDX32>(p, x, yb + j, %s%s);" % (I, zc, args_call))
+            w("            else %s_A<IDX32>(p, x, yb + j, %s%s);" % (I, zc, args_call))
             w("          }")
             w("        } else {")
             w("          for (int y = yb; y < p.hi1; y++) {")
-            w("            if (RESTRICT) %s_R<IDX32>(p, x, y, z%s);" % (I, args_call))
-            w("            else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
+            w("            if (RESTRICT) %s_R<IDX32>(p, x, y, %s%s);" % (I, zc, args_call))
+            w("            else %s_A<IDX32>(p, x, y, %s%s);" % (I, zc, args_call))
             w("          }")
             w("        }")
             w("      }")
+            if hd:
+                w("    }")
             w("  }")
         else:
             # PY points per thread along y (consecutive rows), x / z one each
             w("  const int y0 = p.lo1 + (int)(by * blockDim.y + threadIdx.y) * %d;" % py)
-            w("  const int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z);")
-            if aw is not None:
+            if hd:  # the 3rd to 5th axes as one folded index
+                w("  const int nz = p.hi2 - p.lo2, nu = p.hi3 - p.lo3;")
+                w("  const int zz = (int)(bz * blockDim.z + threadIdx.z);")
+                w("  if (zz >= nz * nu * (p.hi4 - p.lo4)) return;")
+                w("  const int z = p.lo2 + zz % nz, u = p.lo3 + (zz / nz) % nu,"
+                  " v = p.lo4 + zz / (nz * nu);")
+                w("  if (x < p.hi0 && y0 < p.hi1) {")
+                w("    if (RESTRICT) %s_R<IDX32>(p, x, y0, z, u, v%s);" % (I, args_call))
+                w("    else %s_A<IDX32>(p, x, y0, z, u, v%s);" % (I, args_call))
+                w("  }")
+            else:
+                w("  const int z = p.lo2 + (int)(bz * blockDim.z + threadIdx.z);")
+            if hd:
+                pass
+            elif aw is not None:
                 # x starts the row's misalignment (in elements of dat aw)
                 # before lo0, so that a warp's accesses to the rows of aw
                 # begin on 128-byte boundaries; the grid has that many
@@ -1042,7 +1084,9 @@ class Translator:
                 w("  if (x >= p.lo0 && x < p.hi0 && z < p.hi2) {")
             else:
                 w("  if (x < p.hi0 && z < p.hi2) {")
-            if py == 1:
+            if hd:
+                pass
+            elif py == 1:
                 w("    if (y0 < p.hi1) {")
                 w("      if (RESTRICT) %s_R<IDX32>(p, x, y0, z%s);" % (I, args_call))
                 w("      else %s_A<IDX32>(p, x, y0, z%s);" % (I, args_call))
@@ -1062,7 +1106,8 @@ class Translator:
                 w("        else %s_A<IDX32>(p, x, y, z%s);" % (I, args_call))
                 w("      }")
                 w("    }")
-            w("  }")
+            if not hd:
+                w("  }")
         if reds:
             w("  __shared__ double ob2_sh_raw[32 * 2];")
             w("  __shared__ int ob2_flag;")
@@ -1172,6 +1217,8 @@ class Translator:
         w("  memset((void *)&p, 0, sizeof(p));")
         w("  p.lo0 = L.lo[0]; p.lo1 = L.lo[1]; p.lo2 = L.lo[2];")
         w("  p.hi0 = L.hi[0]; p.hi1 = L.hi[1]; p.hi2 = L.hi[2];")
+        if hd:
+            w("  p.lo3 = L.lo4[0]; p.hi3 = L.hi4[0]; p.lo4 = L.lo4[1]; p.hi4 = L.hi4[1];")
         w("  p.counter = L.counter;")
         w("  dim3 blk(L.block[0], L.block[1], L.block[2]);")
         w("  dim3 grd(L.grid[0], L.grid[1], L.grid[2]);")
@@ -1192,6 +1239,9 @@ class Translator:
                   " p.wz%d = L.view[%d].wz;" % (i, p.base_type, i, i, i, i, i, i, i))
                 w("  p.ex%d = L.view[%d].ex; p.ey%d = L.view[%d].ey; p.ez%d = L.view[%d].ez;"
                   " p.ed%d = L.view[%d].ed;" % (i, i, i, i, i, i, i, i))
+                if hd:
+                    w("  p.wu%d = L.view[%d].wu; p.wv%d = L.view[%d].wv; p.eu%d = L.view[%d].eu;"
+                      " p.ev%d = L.view[%d].ev;" % (i, i, i, i, i, i, i, i))
                 if a.prolong:
                     w("  p.mx%d = arg%d.stencil->mgrid_stride[0];" % (i, i))
                     w("  p.my%d = dim > 1 ? arg%d.stencil->mgrid_stride[1] : 1;" % (i, i))
@@ -1224,7 +1274,7 @@ class Translator:
         else:
             w("  const ob2_mlauncher mfn = al ? (L.idx32 ? %s_f_t : %s_f_f)"
               " : (L.idx32 ? %s_t_t : %s_t_f);" % (MN, MN, MN, MN))
-        if not reds:
+        if not reds and not hd:
             w("  L.fuse_id = %d;" % len(self.fuse_items))
             w("  L.ffn = ob2f_launch;")
             w("  L.hfn = L.idx32 ? %s_t : %s_f;" % (HN, HN))

@@ -77,15 +77,21 @@ template <typename T> struct acc_holder {
     }
     const int md = d->dim;
     int sx, sy, sz, sd;
+    // points before the 4th and 5th axes (4D / 5D blocks)
+    const long long c3 = (long long)d->size[0] * d->size[1] * d->size[2];
+    const long long c4 = c3 * d->size[3];
+    int su, sv;
     if (soa) {
       sx = 1; sy = d->size[0]; sz = d->size[0] * d->size[1];
+      su = (int)c3; sv = (int)c4;
       sd = (int)cum;
     } else {
       off *= md;
       sx = md; sy = d->size[0] * md; sz = d->size[0] * d->size[1] * md;
+      su = (int)(c3 * md); sv = (int)(c4 * md);
       sd = 1;
     }
-    a = ACC<T>((T *)d->data + off, sx, sy, sz, sd);
+    a = ACC<T>((T *)d->data + off, sx, sy, sz, su, sv, sd);
   }
   ACC<T> &get() { return a; }
 };
@@ -112,23 +118,25 @@ void run(void (*kernel)(P...), std::index_sequence<I...>, const char *name, ops_
   constexpr int N = sizeof...(P);
   oracle_loop_prologue(name, block, dim, range, args, N);
   std::tuple<typename pick<P>::type...> h;
-  int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
-  for (int i = 0; i < dim && i < 3; i++) {
+  int lo[OPS_MAX_DIM] = {0, 0, 0, 0, 0}, hi[OPS_MAX_DIM] = {1, 1, 1, 1, 1};
+  for (int i = 0; i < dim && i < OPS_MAX_DIM; i++) {
     lo[i] = range[2 * i];
     hi[i] = range[2 * i + 1];
   }
   oracle_dist_loop(name, block, dim, lo, hi, args, N);
   int pt[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
   int gidx[OPS_MAX_DIM] = {0, 0, 0, 0, 0};
-  for (int z = lo[2]; z < hi[2]; z++)
-    for (int y = lo[1]; y < hi[1]; y++)
-      for (int x = lo[0]; x < hi[0]; x++) {
-        pt[0] = x; pt[1] = y; pt[2] = z;
-        gidx[0] = x; gidx[1] = y; gidx[2] = z;
-        (void)std::initializer_list<int>{
-            (std::get<I>(h).set(args[I], gidx, pt, block), 0)...};
-        kernel(std::get<I>(h).get()...);
-      }
+  for (int v = lo[4]; v < hi[4]; v++)
+    for (int u = lo[3]; u < hi[3]; u++)
+      for (int z = lo[2]; z < hi[2]; z++)
+        for (int y = lo[1]; y < hi[1]; y++)
+          for (int x = lo[0]; x < hi[0]; x++) {
+            pt[0] = x; pt[1] = y; pt[2] = z; pt[3] = u; pt[4] = v;
+            gidx[0] = x; gidx[1] = y; gidx[2] = z; gidx[3] = u; gidx[4] = v;
+            (void)std::initializer_list<int>{
+                (std::get<I>(h).set(args[I], gidx, pt, block), 0)...};
+            kernel(std::get<I>(h).get()...);
+          }
   oracle_loop_epilogue(name, block, dim, range, args, N);
 }
 

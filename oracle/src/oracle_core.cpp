@@ -137,8 +137,8 @@ OPS_API void ops_exit(void) {
 }
 
 OPS_API ops_block ops_decl_block(int dims, const char *name) {
-  if (dims < 1 || dims > 3)
-    throw OPSException(OPS_INVALID_ARGUMENT, "Error: ops_decl_block -- dims must be 1..3");
+  if (dims < 1 || dims > OPS_MAX_DIM)
+    throw OPSException(OPS_INVALID_ARGUMENT, "Error: ops_decl_block -- dims must be 1..5");
   ops_block b = (ops_block)calloc(1, sizeof(ops_block_core));
   b->dims = dims;
   b->name = copy_str(name);

@@ -49,6 +49,26 @@ def test_opsunit_parity(args, golden):
         assert_lines_close(got, want, 1e-11)
 
 
+@pytest.mark.parametrize("args", [[], ["-n=9"]])
+def test_hdunit_5d_parity(args):
+    """A 5D block (apps/hdunit): a fill from the point index over the whole
+    storage, a stencil reaching one point along each of the five axes, sum
+    and max reductions over the 5D range (the 3rd to 5th axes folded into
+    the grid's z index), and a halo group flipped along the 4th and 5th
+    axes: every dat bit-exact against the oracle, and the printed sums and
+    maxima equal (their values are sums of dyadic numbers, exact in any
+    order; the oracle's were checked against a numpy restatement)."""
+    gout, gd = run_app("hdunit", "b200", args, dump=True)
+    cout, cd = run_app("hdunit", "oracle", args, dump=True)
+    diffs = compare(gd, cd)
+    assert diffs and max(diffs.values()) == 0.0, diffs
+    g = [l for l in gout.splitlines() if l.startswith("hdunit")]
+    c = [l for l in cout.splitlines() if l.startswith("hdunit")]
+    assert len(g) == 2 and g == c, (g, c)
+    if not args:
+        assert g[0] == "hdunit sums 63731.25 max 107.34375", g
+
+
 def test_poisson_mb_parity_and_reference(golden):
     gout, gd = run_app("poisson_mb", "b200", dump=True)
     cout, cd = run_app("poisson_mb", "oracle", dump=True)
@@ -196,6 +216,8 @@ REF_APPS = [
     ("ref_halfprecision", [], "half", "This run is considered PASSED"),
     ("ref_lbm", [], "exact", "Test PASSED"),
     ("ref_tiling_fix", [], "exact", ""),
+    # 4D blocks: par_loops over 4D ranges with ops_arg_idx, a 4D halo group
+    ("ref_mblock4d", [], "exact", "Total Wall time"),
 ]
 
 
