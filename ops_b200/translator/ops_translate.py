@@ -987,6 +987,12 @@ class Translator:
             w("  %s(%s);" % (loop.kernel, ", ".join(call)))
             w("}")
         py = 1 if hd else self.rows_per_thread(dats, kd)
+        # a 3D loop whose extra rows per thread come only from its narrow
+        # elements (not from stencil reuse along y) takes one row per thread
+        # with 128-byte row alignment instead
+        if (not hd and loop.ndim == 3 and not reds and py > 1 and not self.py_forced and
+                not self.light_y_stencil(kd) and self.align_dat(loop, kd, dats, reds, 1) is not None):
+            py = 1
         aw = self.align_dat(loop, kd, dats, reds, py)
         if aw is not None:
             w("template <bool RESTRICT, bool IDX32, bool ALIGN = true>")
