@@ -192,6 +192,7 @@ def _deps(name: str, flavour: str):
             deps += [os.path.join(dd, f) for f in os.listdir(dd) if f.endswith(".h")]
     if flavour == "b200":
         deps.append(os.path.join(ROOT, "ops_b200", "translator", "ops_translate.py"))
+        deps.append(os.path.join(ROOT, "ops_b200", "translator", "divrewrite.py"))
         deps.append(os.path.join(ROOT, "ops_b200", "build_app.py"))
         inc = os.path.join(ROOT, "include")
         deps += [os.path.join(inc, f) for f in os.listdir(inc)]

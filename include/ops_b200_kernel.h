@@ -250,6 +250,79 @@ __device__ __forceinline__ void hfuse_prologue(const ob2_hfuse &h, int inst, int
   }
 }
 
+/* ---- division in user kernels -------------------------------------------
+ * The translator rewrites every binary `/` of a user kernel it can parse
+ * safely into div(lhs, rhs) (ops_b200/translator/divrewrite.py).  A double
+ * quotient is computed by ddiv, every other quotient by the operator itself.
+ *
+ * Why: CUDA's double division takes a long guarded path when the numerator
+ * is zero (measured on the B200, 7 divisions per point over 16M points:
+ * 109 us with nonzero numerators, 332 us with zero ones), and hydrodynamics
+ * kernels divide zero gradients and fluxes on every cell at rest.  ddiv
+ * costs the same for both (129-135 us).
+ *
+ * ddiv(a, b) returns the correctly rounded quotient, the same bits as the
+ * IEEE division, by Newton-Raphson iteration on the reciprocal and
+ * Markstein's correction of the quotient (P. Markstein, "Computation of
+ * elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+ * Dev. 34(1), 1990; the theorems as stated in J.-M. Muller et al., Handbook
+ * of Floating-Point Arithmetic, ch. 4-5):
+ *   y0 = the hardware reciprocal approximation of b (rcp.approx.ftz.f64);
+ *   y <- y + y (1 - b y), three times with fused multiply-adds: two steps
+ *        bring y within one ulp of 1/b, and the third then rounds it
+ *        correctly (Markstein's reciprocal theorem; it excludes divisors
+ *        whose significand is all ones, which take the IEEE division here);
+ *   q0 = RN(a y) is within one ulp of a/b; r = a - b q0 is exact with an
+ *        FMA; q = RN(q0 + r y) is RN(a/b) (Markstein's division theorem).
+ * The theorems need every intermediate in the normal range: |a| and |b| in
+ * [2^-500, 2^500) guarantee that (the quotient, the residual and the
+ * reciprocal stay far from underflow and overflow).  Zero numerators return
+ * RN(a y), the correctly signed zero.  Every other operand (subnormal, huge,
+ * zero divisor, infinity, NaN) takes the IEEE division.  Checked against
+ * CUDA's `/` bit for bit on 10^10 generated pairs (tests/test_gpu_ddiv.py).
+ * A zero-numerator shortcut in front of the IEEE division was measured as
+ * well and was slower inside the CloverLeaf kernels (5.27 against 4.79 ms
+ * per 3840^2 step). */
+__device__ __forceinline__ double ddiv(double a, double b) {
+  const unsigned ha = (unsigned)__double2hiint(a), hb = (unsigned)__double2hiint(b);
+  const unsigned ea = (ha >> 20) & 0x7ffu, eb = (hb >> 20) & 0x7ffu;
+  const bool b_ok = (eb - 523u < 1000u) &&
+                    !((hb & 0xfffffu) == 0xfffffu && __double2loint(b) == -1);
+  const bool a_ok = (ea - 523u < 1000u) || a == 0.0;
+  if (!(a_ok && b_ok)) return a / b;
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  const double q0 = __dmul_rn(a, y);
+  const double r = __fma_rn(-b, q0, a);
+  return a == 0.0 ? q0 : __fma_rn(r, y, q0);
+}
+
+template <typename A, typename B>
+using quot_t = decltype(std::declval<A>() / std::declval<B>());
+
+/* quotients that are not double: the operator itself (constexpr, so a
+ * rewritten integer division still works in a constant expression) */
+template <typename A, typename B,
+          typename std::enable_if<!std::is_same<quot_t<A, B>, double>::value,
+                                        int>::type = 0>
+__host__ __device__ constexpr quot_t<A, B> div(A a, B b) {
+  return a / b;
+}
+
+/* double quotients (after the usual arithmetic conversions) */
+template <typename A, typename B,
+          typename std::enable_if<std::is_same<quot_t<A, B>, double>::value,
+                                        int>::type = 0>
+__device__ __forceinline__ double div(A a, B b) {
+  return ddiv((double)a, (double)b);
+}
+
 }  // namespace ob2
 
 #endif /* OPS_B200_KERNEL_H */

@@ -33,6 +33,8 @@ import sys
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
 
+from .divrewrite import macro_table, rewrite_divisions
+
 # --------------------------------------------------------------------------
 # scanning helpers
 # --------------------------------------------------------------------------
@@ -331,6 +333,11 @@ class Translator:
         # element instead of being made
         self.check = os.environ.get("OPS_B200_CHECK", "0") == "1"
         self.minb = max(0, int(os.environ.get("OPS_B200_MINB", "4")))
+        # OPS_B200_DDIV=0: user kernels keep their `/` operators; otherwise
+        # every division the scanner can group safely becomes ob2::div
+        # (include/ops_b200_kernel.h: correctly rounded, the same bits)
+        self.ddiv = os.environ.get("OPS_B200_DDIV", "1") != "0"
+        self.div_counts = [0, 0]
 
     # -- discovery ---------------------------------------------------------
     def resolve_include(self, name: str, from_dir: str) -> Optional[str]:
@@ -558,8 +565,33 @@ class Translator:
             if idx:
                 legacy[loop.kernel] = (loop.ndim, idx)
 
+        macros = None
+        if self.ddiv:
+            texts = []
+            for f in list(self.sources) + list(self.headers) + [
+                    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+                        os.path.abspath(__file__)))), "include", "ops_lib_core.h")]:
+                try:
+                    texts.append(open(f).read())
+                except OSError:
+                    pass
+            macros = macro_table(texts)
+
+        def divisions(text: str) -> str:
+            """the function with its body's divisions rewritten"""
+            if macros is None:
+                return text
+            masked = mask_comments_strings(text)
+            lb = masked.find("{")
+            if lb < 0:
+                return text
+            body, done, kept = rewrite_divisions(text[lb:], mask_comments_strings, macros)
+            self.div_counts[0] += done
+            self.div_counts[1] += kept
+            return text[:lb] + body
+
         def emit_fn(kd):
-            text = re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text)
+            text = divisions(re.sub(r"^\s*(static\s+|inline\s+)*", "", kd.text))
             if kd.name not in legacy:
                 if re.search(r"\bOPS_ACC(_MD)?\d+\s*\(", mask_comments_strings(text)):
                     return  # an OPS_ACCn kernel no loop of this program calls
@@ -636,6 +668,8 @@ class Translator:
           " ob2_register_const_handler(&ob2_const_copy); } };")
         w("static ob2_const_registrar ob2_const_registrar_instance;")
         w("}  // namespace")
+        L.insert(1, "/* divisions in user kernels: %d as ob2::div, %d kept as written */" %
+                 tuple(self.div_counts))
         with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
             f.write("\n".join(L) + "\n")
 

@@ -168,3 +168,63 @@ def test_fused_dispatcher_ids_name_each_loops_own_body():
     for name, k in ids.items():
         assert k in cases, (name, k)
         assert cases[k][0] == "ob2b_" + name and cases[k][1].startswith("ob2p_"), (name, cases[k])
+
+
+DIV_CASES = [
+    "a * b / c", "a / b * c", "-a / b", "a / -b", "a + b * c / d - e", "a / b / c",
+    "(double)i / n", "f1(a) / (b + c)", "MIN(a / b, c)", "SIGN(a / b, c)", "a / SQ(b)",
+    "BAD / c", "K / c", "p->x / s.y[1]", "c > 0 ? a / b : d / e", "*q / 2", "0.5*(a-b)/c",
+    "a /* note */ / b", "(double)(a) / b", "-a * b / c / d * e", "a * -b / c", "d / 3",
+    "i / j * a", "a / i / j", "2 * a / 3.0 + b / -c", "(a + b) / (c - d) / e",
+]
+
+
+def test_division_rewrite_keeps_the_grouping():
+    """Every rewritten expression, with ob2::div defined as the operator
+    itself, evaluates to the same bits as the original on random values: the
+    rewrite chose the operands C's grammar gives each `/` (a wrong grouping
+    changes the rounding, or the integer quotient, on almost every sample)."""
+    from ops_b200.translator.divrewrite import macro_table, rewrite_divisions
+    macros = macro_table([open(os.path.join(ROOT, "include", "ops_lib_core.h")).read(),
+                          "#define SQ(x) x*x\n#define K 3.0\n#define BAD a+b\n"])
+    rewritten = []
+    n_done = 0
+    for e in DIV_CASES:
+        r, done, _ = rewrite_divisions("{ return " + e + "; }", mask_comments_strings, macros)
+        n_done += done
+        rewritten.append(r[len("{ return "):-len("; }")])
+    assert rewritten[0] == "::ob2::div(a * b, c)" and rewritten[1] == "::ob2::div(a, b) * c"
+    assert rewritten[10] == "a / SQ(b)" and rewritten[11] == "BAD / c"  # unsafe macros kept
+    assert rewritten[18] == "(double)(a) / b"  # a cast of a group is not parsed: kept
+    assert n_done >= 29
+    src = ["#include <cstdio>", "#include <cstring>", "#include <cstdlib>",
+           '#include "ops_lib_core.h"',
+           "namespace ob2 { template <class A, class B> auto div(A a, B b) { return a / b; } }",
+           "#define SQ(x) x*x", "#define K 3.0", "#define BAD a+b",
+           "struct P { double x; double y[2]; };",
+           "static double f1(double v) { return v * 1.5; }"]
+    args = "double a, double b, double c, double d, double e, int i, int j, int n, P *p, P s, double *q"
+    for k, (o, r) in enumerate(zip(DIV_CASES, rewritten)):
+        src.append("static double o%d(%s) { return %s; }" % (k, args, o))
+        src.append("static double r%d(%s) { return %s; }" % (k, args, r))
+    src.append("int main() { srand(7); int bad = 0;")
+    src.append(" for (int t = 0; t < 20000; t++) {")
+    src.append("  double v[5]; for (int m = 0; m < 5; m++) v[m] = (rand() - RAND_MAX / 2) /"
+               " (double)(rand() % 997 + 1) + 1e-3;")
+    src.append("  int i = rand() % 200 - 100, j = rand() % 13 + 1, n = rand() % 50 + 1;")
+    src.append("  P pp = {v[1] * 3.7, {v[2] * 0.3, v[3] * 1.9}}; double qq = v[4] * 7.1;")
+    for k in range(len(DIV_CASES)):
+        src.append("  { double x = o%d(v[0], v[1], v[2], v[3], v[4], i, j, n, &pp, pp, &qq),"
+                   " y = r%d(v[0], v[1], v[2], v[3], v[4], i, j, n, &pp, pp, &qq);"
+                   " if (memcmp(&x, &y, 8)) { if (bad < 5) printf(\"case %d\\n\"); bad++; } }"
+                   % (k, k, k))
+    src.append(" }")
+    src.append(" printf(\"bad %d\\n\", bad); return bad != 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.cpp")
+        open(c, "w").write("\n".join(src) + "\n")
+        exe = os.path.join(d, "t")
+        subprocess.run(["g++", "-std=c++17", "-O1", "-ffp-contract=off", "-I",
+                        os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        r = subprocess.run([exe], capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout
