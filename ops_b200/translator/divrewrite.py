@@ -206,7 +206,9 @@ class _Scan:
         s = self.postfix_start(e)
         while True:
             p = s - 1
-            if self.s(p) in PREFIX_OPS and self.s(p) not in ("++", "--"):
+            if self.s(p) in ("++", "--", "sizeof", "alignof", "new", "delete"):
+                raise _Fail()  # these bind to the operand, not to the quotient
+            if self.s(p) in PREFIX_OPS:
                 if self.ends_operand(p - 1):
                     return s  # a binary operator: the unary expression ends here
                 if self.s(p - 1) in ("++", "--"):

@@ -196,6 +196,9 @@ def test_division_rewrite_keeps_the_grouping():
     assert rewritten[0] == "::ob2::div(a * b, c)" and rewritten[1] == "::ob2::div(a, b) * c"
     assert rewritten[10] == "a / SQ(b)" and rewritten[11] == "BAD / c"  # unsafe macros kept
     assert rewritten[18] == "(double)(a) / b"  # a cast of a group is not parsed: kept
+    for kept in ("sizeof x / y", "++i / 2", "--i / 2", "sizeof(double) / 2"):
+        r, done, _ = rewrite_divisions("{ " + kept + "; }", mask_comments_strings, macros)
+        assert done == 0 and r == "{ " + kept + "; }", r
     assert n_done >= 29
     src = ["#include <cstdio>", "#include <cstring>", "#include <cstdlib>",
            '#include "ops_lib_core.h"',
