@@ -49,6 +49,13 @@ struct KStat {
   int best[3] = {0, 0, 0};
   std::vector<void *> tune_ev;        // start/end event per candidate
   std::vector<long long> tune_pts;    // points of the candidate's launch
+  // temporal-blocking depth autotuning (OPS_B200_TB_DEPTH=auto): 0 trying the
+  // candidates, 1 every candidate timed, 2 decided (tb_best sweeps per launch)
+  int tb_state = 0;
+  int tb_next = 0;
+  int tb_best = 0;
+  std::vector<void *> tb_ev;          // start/end event per timed chain
+  std::vector<long long> tb_sw;       // sweeps of the timed chain
 };
 
 // block shapes the autotuner tries (x, y, z); one thread per point, so the
@@ -198,6 +205,7 @@ struct Runtime {
   // depths 2 / 4 / 8 against 272 GLUPS sweep by sweep
   bool tb = false;
   int tb_depth = 8;           // sweeps per temporal-blocking launch (OPS_B200_TB_DEPTH)
+  bool tb_auto = false;       // OPS_B200_TB_DEPTH=auto: depth chosen per loop by timing
   long long tb_launches = 0, tb_sweeps = 0;
   std::vector<std::array<long long, 3>> *rename_log = nullptr;  // while capturing
 };
@@ -1017,8 +1025,94 @@ void tb_rename(ops_dat d, char *now) {
   x.spare = old;
 }
 
+/* Temporal-blocking depth autotuner (OPS_B200_TB_DEPTH=auto).  The first
+ * chains of a loop's ping-pong sweeps run outside graphs, each with one of
+ * the candidate depths (1: plain sweeps, no blocking) and bracketed by
+ * events, kTbReps times per candidate; at the next flush the depth with the
+ * least device time per sweep is kept for the rest of the run, and chains of
+ * that loop are captured into graphs again.  Every depth computes every
+ * point with the same code on the same values, so the choice changes no
+ * result. */
+constexpr int kTbDepths[] = {1, 2, 4, 8};
+constexpr int kTbCands = (int)(sizeof kTbDepths / sizeof kTbDepths[0]);
+constexpr int kTbReps = 2;
+
+void tb_decide(KStat &k) {
+  std::vector<double> best(kTbCands, 1e300);
+  for (int c = 0; c < kTbCands * kTbReps && 2 * c + 1 < (int)k.tb_ev.size(); c++) {
+    float ms = 0.f;
+    if (!k.tb_ev[2 * c] || ob2_event_elapsed_ms(k.tb_ev[2 * c], k.tb_ev[2 * c + 1], &ms)) continue;
+    best[c % kTbCands] =
+        std::min(best[c % kTbCands], ms / (double)std::max(1LL, k.tb_sw[c]));
+  }
+  int bi = 0;
+  for (int c = 1; c < kTbCands; c++)
+    if (best[c] < best[bi]) bi = c;
+  k.tb_best = kTbDepths[bi];
+  for (void *e : k.tb_ev)
+    if (e) rt().ev_pool.push_back(e);
+  k.tb_ev.clear();
+  k.tb_sw.clear();
+  k.tb_state = 2;
+}
+
+// true when the queue holds a ping-pong chain whose depth is still being
+// tuned (the flush then runs it outside a graph, timed); decides the loops
+// whose candidates have all been timed
+bool tb_tuning(std::vector<Runtime::QItem> &q) {
+  Runtime &r = rt();
+  if (!r.tb_auto) return false;
+  for (size_t i = 0; i < q.size(); i++) {
+    if (q[i].kind != 0 || !q[i].tfn) continue;
+    const size_t j = tb_chain(q, i);
+    if (j - i < 2) continue;
+    KStat &k = r.kstats[q[i].kidx];
+    if (k.tb_state == 1) {
+      check(ob2_dev_sync(), "temporal-blocking depth tuning");
+      tb_decide(k);
+    }
+    if (k.tb_state == 0) return true;
+    i = j - 1;
+  }
+  return false;
+}
+
+int tb_depth_of(const Runtime::QItem &F) {
+  Runtime &r = rt();
+  if (!r.tb_auto) return r.tb_depth;
+  const KStat &k = r.kstats[F.kidx];
+  return k.tb_state == 2 ? k.tb_best : kTbDepths[k.tb_next % kTbCands];
+}
+
+void run_tb_sweeps(std::vector<Runtime::QItem> &q, size_t i, size_t j, int depth);
+
 void run_tb(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
   Runtime &r = rt();
+  const int depth = tb_depth_of(q[i]);
+  KStat &k = r.kstats[q[i].kidx];
+  const bool timed = r.tb_auto && k.tb_state == 0 && !r.capturing;
+  void *e0 = nullptr;
+  if (timed) {
+    e0 = pool_event();
+    check(ob2_event_record(e0), "event");
+  }
+  run_tb_sweeps(q, i, j, depth);
+  if (timed) {
+    void *e1 = pool_event();
+    check(ob2_event_record(e1), "event");
+    k.tb_ev.push_back(e0);
+    k.tb_ev.push_back(e1);
+    k.tb_sw.push_back((long long)(j - i));
+    if (++k.tb_next == kTbCands * kTbReps) k.tb_state = 1;
+  }
+}
+
+void run_tb_sweeps(std::vector<Runtime::QItem> &q, size_t i, size_t j, int depth) {
+  Runtime &r = rt();
+  if (depth < 2) {  // plain sweeps: every item as queued
+    for (size_t a = i; a < j; a++) run_item(q[a], nullptr, nullptr);
+    return;
+  }
   size_t a = i;
   while (a < j) {
     int ks = -1, kw = -1;
@@ -1030,7 +1124,7 @@ void run_tb(std::vector<Runtime::QItem> &q, size_t i, size_t j) {
       run_item(q[a], nullptr, nullptr);  // one sweep left: as it is
       break;
     }
-    const size_t b = std::min(j, a + (size_t)r.tb_depth);
+    const size_t b = std::min(j, a + (size_t)depth);
     Runtime::QItem &F = q[a];
     ops_dat X = r.dats[F.acc[ks].dat];
     DatX &xx = r.datx[X->index];
@@ -1129,7 +1223,8 @@ OPS_API void ob2_flush(void) {
   std::vector<Runtime::QItem> q;
   q.swap(r.q);
   r.chains++;
-  if (!r.graphs || r.ktime) {  // per-kernel event timing needs plain launches
+  // per-kernel event timing and depth tuning need plain launches
+  if (!r.graphs || r.ktime || tb_tuning(q)) {
     tb_prepare(q);
     run_queue(q);
     return;
@@ -1473,7 +1568,12 @@ OPS_API void ops_init(const int argc, const char *const argv[], const int diags)
   if ((e = getenv("OPS_B200_FUSE"))) r.fuse = atoi(e) != 0;
   if ((e = getenv("OPS_B200_HFUSE"))) r.hfuse = atoi(e) != 0;
   if ((e = getenv("OPS_B200_TB"))) r.tb = atoi(e) != 0;
-  if ((e = getenv("OPS_B200_TB_DEPTH"))) r.tb_depth = std::max(2, std::min(OB2_TB_MAX, atoi(e)));
+  if ((e = getenv("OPS_B200_TB_DEPTH"))) {
+    if (!strcmp(e, "auto"))
+      r.tb_auto = true;
+    else
+      r.tb_depth = std::max(2, std::min(OB2_TB_MAX, atoi(e)));
+  }
   if ((e = getenv("OPS_B200_FUSE_PTS"))) r.fuse_pts = atoll(e);
   if ((e = getenv("OPS_B200_TUNE_FILE")) && *e) {
     r.tune_file = e;
@@ -2558,6 +2658,15 @@ OPS_API size_t ops_timing_output_str(char *buf, size_t n) {
       if (k.tune_state == 2) {
         snprintf(line, sizeof line, " %s=%dx%dx%d", k.name.c_str(), k.best[0], k.best[1],
                  k.best[2]);
+        s += line;
+      }
+    s += "\n";
+  }
+  if (r.tb_auto) {
+    s += "  Temporal-blocking depths (1: plain sweeps):";
+    for (auto &k : r.kstats)
+      if (k.tb_state == 2) {
+        snprintf(line, sizeof line, " %s=%d", k.name.c_str(), k.tb_best);
         s += line;
       }
     s += "\n";

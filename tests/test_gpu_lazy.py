@@ -98,6 +98,23 @@ def test_temporal_blocking_matches_eager(depth, args):
     assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
 
 
+def test_temporal_blocking_depth_autotuned():
+    """OPS_B200_TB_DEPTH=auto: the first chains of the Jacobi sweeps run with
+    each candidate depth (1 = plain sweeps, 2, 4, 8) outside graphs and timed,
+    then one depth is kept; every dat and printed residual still equal eager
+    execution bit for bit, and the run reports the depth it chose."""
+    args = ["-nb=1", "-n=257", "-sweeps=1100", "-check=0"]
+    eo, ed = run_app("poisson_mb", "b200", args, dump=True, env=EAGER)
+    lo, ld = run_app("poisson_mb", "b200", args, dump=True,
+                     env={"OPS_B200_LAZY": "1", "OPS_B200_TB": "1", "OPS_B200_TB_DEPTH": "auto"})
+    m = re.search(r"Temporal-blocking depths \(1: plain sweeps\):((?: \S+=\d+)+)", lo)
+    assert m, lo[-800:]
+    depths = [int(x.split("=")[1]) for x in m.group(1).split()]
+    assert depths and all(d in (1, 2, 4, 8) for d in depths), m.group(0)
+    same(ld, ed)
+    assert numbers_only(result_lines(lo)) == numbers_only(result_lines(eo))
+
+
 @pytest.mark.parametrize("mode", ["lazy_graphs", "tiled_graphs", "tiled_cache"])
 def test_cloverleaf_lazy_matches_eager(tmp_path, mode):
     ensure("clover_step", "b200")
