@@ -176,6 +176,7 @@ DIV_CASES = [
     "BAD / c", "K / c", "p->x / s.y[1]", "c > 0 ? a / b : d / e", "*q / 2", "0.5*(a-b)/c",
     "a /* note */ / b", "(double)(a) / b", "-a * b / c / d * e", "a * -b / c", "d / 3",
     "i / j * a", "a / i / j", "2 * a / 3.0 + b / -c", "(a + b) / (c - d) / e",
+    "SCALE(a / b)", "MAX(a / b, c / d) / e",
 ]
 
 
@@ -186,7 +187,8 @@ def test_division_rewrite_keeps_the_grouping():
     changes the rounding, or the integer quotient, on almost every sample)."""
     from ops_b200.translator.divrewrite import macro_table, rewrite_divisions
     macros = macro_table([open(os.path.join(ROOT, "include", "ops_lib_core.h")).read(),
-                          "#define SQ(x) x*x\n#define K 3.0\n#define BAD a+b\n"])
+                          "#define SQ(x) x*x\n#define K 3.0\n#define BAD a+b\n"
+                          "#define SCALE(v) 2.0*v\n"])
     rewritten = []
     n_done = 0
     for e in DIV_CASES:
@@ -196,6 +198,9 @@ def test_division_rewrite_keeps_the_grouping():
     assert rewritten[0] == "::ob2::div(a * b, c)" and rewritten[1] == "::ob2::div(a, b) * c"
     assert rewritten[10] == "a / SQ(b)" and rewritten[11] == "BAD / c"  # unsafe macros kept
     assert rewritten[18] == "(double)(a) / b"  # a cast of a group is not parsed: kept
+    # SCALE puts its argument after a `*`: a division passed to it is kept
+    assert rewritten[26] == "SCALE(a / b)"
+    assert rewritten[27] == "::ob2::div(MAX(::ob2::div(a, b), ::ob2::div(c, d)), e)"
     for kept in ("sizeof x / y", "++i / 2", "--i / 2", "sizeof(double) / 2"):
         r, done, _ = rewrite_divisions("{ " + kept + "; }", mask_comments_strings, macros)
         assert done == 0 and r == "{ " + kept + "; }", r
@@ -203,7 +208,7 @@ def test_division_rewrite_keeps_the_grouping():
     src = ["#include <cstdio>", "#include <cstring>", "#include <cstdlib>",
            '#include "ops_lib_core.h"',
            "namespace ob2 { template <class A, class B> auto div(A a, B b) { return a / b; } }",
-           "#define SQ(x) x*x", "#define K 3.0", "#define BAD a+b",
+           "#define SQ(x) x*x", "#define K 3.0", "#define BAD a+b", "#define SCALE(v) 2.0*v",
            "struct P { double x; double y[2]; };",
            "static double f1(double v) { return v * 1.5; }"]
     args = "double a, double b, double c, double d, double e, int i, int j, int n, P *p, P s, double *q"
