@@ -236,3 +236,62 @@ def test_division_rewrite_keeps_the_grouping():
                         os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         r = subprocess.run([exe], capture_output=True, text=True)
         assert r.returncode == 0, r.stdout
+
+
+def test_markstein_division_steps_round_correctly_on_the_host():
+    """The steps of ob2::ddiv (include/ops_b200_kernel.h) restated on the
+    host with a poorer start than the GPU's (the float reciprocal, about 24
+    bits, in place of rcp.approx.ftz.f64): three Newton-Raphson steps on the
+    reciprocal, then Markstein's quotient correction, all with fused
+    multiply-adds, equal the IEEE quotient on random operands of the fast
+    domain (both in [2^-500, 2^500)), near-midpoint quotients and zero
+    numerators.  The GPU test (tests/test_gpu_ddiv.py) checks the device
+    code itself against CUDA's `/`."""
+    src = r'''
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+static uint64_t st = 88172645463325252ull;
+static uint64_t rnd() { st ^= st << 13; st ^= st >> 7; st ^= st << 17; return st; }
+static double with_exp(uint64_t bits, unsigned e) {
+  bits = (bits & 0x800fffffffffffffull) | ((uint64_t)e << 52);
+  double d; memcpy(&d, &bits, 8); return d;
+}
+static double ddiv(double a, double b) {
+  double y = (double)(1.0f / (float)b);
+  double e = std::fma(-b, y, 1.0); y = std::fma(y, e, y);
+  e = std::fma(-b, y, 1.0); y = std::fma(y, e, y);
+  e = std::fma(-b, y, 1.0); y = std::fma(y, e, y);
+  const double q0 = a * y, r = std::fma(-b, q0, a);
+  return a == 0.0 ? q0 : std::fma(r, y, q0);
+}
+int main() {
+  long bad = 0, n = 0;
+  for (int mode = 0; mode < 3; mode++)
+    for (int t = 0; t < 2000000; t++) {
+      double a, b;
+      const uint64_t r0 = rnd(), r1 = rnd(), r2 = rnd();
+      b = with_exp(r1, 1023 - 100 + (unsigned)(r2 % 200));
+      if ((r1 & 0xfffffffffffffull) == 0xfffffffffffffull) continue;  // all-ones: IEEE path
+      if (mode == 0) a = with_exp(r0, 523 + (unsigned)((r2 >> 20) % 1000));
+      else if (mode == 1) {
+        const double q = std::fabs(with_exp(r0, 1023 + (unsigned)((r2 >> 20) % 64) - 32));
+        a = std::fma(b, q, b * std::ldexp(std::fabs(q), -53));  // q + half an ulp, times b
+      } else a = (r0 & 1) ? -0.0 : 0.0;
+      const double want = a / b, got = ddiv(a, b);
+      n++;
+      if (memcmp(&want, &got, 8)) { if (bad < 3) printf("%a / %a: %a vs %a\n", a, b, got, want); bad++; }
+    }
+  printf("%ld of %ld differ\n", bad, n);
+  return bad != 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "m.cpp")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "m")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-mfma", c, "-o", exe],
+                       check=True)
+        r = subprocess.run([exe], capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout
