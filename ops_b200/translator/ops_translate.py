@@ -669,7 +669,8 @@ class Translator:
         w("static ob2_const_registrar ob2_const_registrar_instance;")
         w("}  // namespace")
         L.insert(1, "/* divisions in user kernels: %d as ob2::div, %d kept as written */" %
-                 tuple(self.div_counts))
+                 tuple(self.div_counts) if self.ddiv else
+                 "/* divisions in user kernels: all kept as written (OPS_B200_DDIV=0) */")
         with open(os.path.join(self.outdir, self.app + "_kernels.cu"), "w") as f:
             f.write("\n".join(L) + "\n")
 

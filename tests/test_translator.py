@@ -68,6 +68,17 @@ def test_translate_and_compile_opsunit():
         assert "ob2i_%s_R" % k in cu and "ob2i_%s_A" % k in cu
     assert "__restrict__" in cu and "__constant__ double ou_scale;" in cu
     assert "ob2::final_combine<double, OPS_MIN>" in cu
+    # the kernels' divisions go through ob2::div (compiled below), unless
+    # OPS_B200_DDIV=0 at translation time
+    assert "::ob2::div(" in cu and "1 as ob2::div, 0 kept as written" in cu
+    out0 = tempfile.mkdtemp(prefix="tr0_")
+    os.environ["OPS_B200_DDIV"] = "0"
+    try:
+        Translator([src], [], "opsunit", out0).run()
+    finally:
+        del os.environ["OPS_B200_DDIV"]
+    cu0 = open(os.path.join(out0, "opsunit_kernels.cu")).read()
+    assert "::ob2::div(" not in cu0 and "all kept as written (OPS_B200_DDIV=0)" in cu0
     ops = open(os.path.join(out, "opsunit_ops.cpp")).read()
     assert "ops_par_loop(" not in ops.replace("ops_par_loop_", "")
     # compile the kernels for sm_100a (cross-compiles without a GPU)
